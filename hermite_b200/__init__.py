@@ -1,0 +1,233 @@
+"""hermite_b200 -- B200-native Hermite N-body force calculator.
+
+Python mirror of the reference's force-calculator interface (`struct Gravity`
+of SRC/hermite{4,6,8}-titan.h, driven by SRC/nbodysystem.h), over the C ABI of
+libhermite_b200.so (include/hermite_b200.h):
+
+    g = Gravity(order=6, nbody=N, precision="mixed")
+    g.set_jp_records(records)               # or g.set_jp(addr, ...)
+    g.predict_all(tsys)
+    force = g.calc_force_on_first_nact(nact, eps2)     # (nact, 3*(order/2))
+    pot = g.calc_potential(eps2)                        # (N,)
+
+Record layouts are those of the reference's CUDA path:
+  j-particle record (8 + 3*(order-2) doubles):
+      pos[3] mass vel[3] tlast acc[3] jrk[3] [snp[3] crk[3]] [d4a[3] d5a[3]]
+  force record (3*(order/2) doubles): acc[3] jrk[3] [snp[3]] [crk[3]]
+
+There is no CPU fallback: if the CUDA library is missing or no sm_100 device
+is present, constructing a Gravity raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = ["Gravity", "HermiteError", "record_words", "force_words", "FP64", "MIXED",
+           "library_path", "load_library", "measure_fma_peak", "EXPORTED_SYMBOLS"]
+
+FP64 = 0
+MIXED = 1
+_PREC = {"fp64": FP64, "mixed": MIXED, FP64: FP64, MIXED: MIXED}
+
+_PKG = Path(__file__).resolve().parent
+_LIB_PATH = _PKG / "_lib" / "libhermite_b200.so"
+_lib = None
+
+# Every entry point declared in include/hermite_b200.h.
+EXPORTED_SYMBOLS = (
+    "hb_create", "hb_destroy", "hb_set_jp", "hb_set_jp_records", "hb_predict_all",
+    "hb_force_first_nact", "hb_potential", "hb_set_precision", "hb_get_precision",
+    "hb_last_error", "hb_status_string", "hb_set_stream", "hb_upload",
+    "hb_predict_all_device", "hb_force_device", "hb_download_forces", "hb_device_forces",
+    "hb_synchronize", "hb_launch_count", "hb_set_force_shape", "hb_force_variant_count",
+    "hb_force_variant_info", "hb_measure_fma_peak",
+)
+
+
+def record_words(order: int) -> int:
+    return 8 + 3 * (order - 2)
+
+
+def force_words(order: int) -> int:
+    return 3 * (order // 2)
+
+
+class HermiteError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("HERMITE_B200_LIB", _LIB_PATH))
+
+
+def load_library() -> ctypes.CDLL:
+    """Load libhermite_b200.so (built by `python -m hermite_b200.build`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not path.exists():
+        raise RuntimeError(f"{path} is missing: build it with `python -m hermite_b200.build`")
+    lib = ctypes.CDLL(str(path))
+    P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    dp = ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "hb_create": (I, [I, I, I, ctypes.POINTER(P)]),
+        "hb_destroy": (I, [P]),
+        "hb_set_jp": (I, [P, I, dp, D, dp, D, dp]),
+        "hb_set_jp_records": (I, [P, I, I, dp]),
+        "hb_predict_all": (I, [P, D]),
+        "hb_force_first_nact": (I, [P, I, D, dp]),
+        "hb_potential": (I, [P, D, dp]),
+        "hb_set_precision": (I, [P, I]),
+        "hb_get_precision": (I, [P]),
+        "hb_last_error": (ctypes.c_char_p, [P]),
+        "hb_status_string": (ctypes.c_char_p, [I]),
+        "hb_set_stream": (I, [P, P]),
+        "hb_upload": (I, [P]),
+        "hb_predict_all_device": (I, [P, D]),
+        "hb_force_device": (I, [P, I, D]),
+        "hb_download_forces": (I, [P, I, dp]),
+        "hb_device_forces": (P, [P]),
+        "hb_synchronize": (I, [P]),
+        "hb_launch_count": (ctypes.c_longlong, [P]),
+        "hb_set_force_shape": (I, [P, I, I]),
+        "hb_force_variant_count": (I, [I, I]),
+        "hb_force_variant_info": (I, [I, I, I, ctypes.POINTER(I), ctypes.POINTER(I),
+                                      ctypes.POINTER(I)]),
+        "hb_measure_fma_peak": (I, [I, dp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    _lib = lib
+    return lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def measure_fma_peak(mode: int) -> float:
+    """Measured FMA-pipe peak in GFLOP/s: mode 0 FP64, 1 FP32, 2 packed FP32."""
+    lib = load_library()
+    out = ctypes.c_double(0.0)
+    st = lib.hb_measure_fma_peak(mode, ctypes.byref(out))
+    if st != 0:
+        raise HermiteError(st, lib.hb_status_string(st).decode())
+    return out.value
+
+
+class Gravity:
+    """The reference's `struct Gravity`, one CUDA context-owned instance."""
+
+    def __init__(self, order: int, nbody: int, precision="fp64"):
+        self._lib = load_library()
+        self.order, self.nbody = int(order), int(nbody)
+        self.R, self.F = record_words(self.order), force_words(self.order)
+        h = ctypes.c_void_p()
+        st = self._lib.hb_create(self.order, self.nbody, _PREC[precision], ctypes.byref(h))
+        if st != 0:
+            raise HermiteError(st, f"hb_create(order={order}, nbody={nbody}): "
+                                   + self._lib.hb_status_string(st).decode())
+        self._h = h
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, st: int, what: str):
+        if st != 0:
+            msg = self._lib.hb_last_error(self._h).decode() or self._lib.hb_status_string(st).decode()
+            raise HermiteError(st, f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    # -- the reference interface -----------------------------------------
+    def set_jp(self, addr: int, pos, mass: float, vel, tlast: float, derivs):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        derivs = np.ascontiguousarray(derivs, dtype=np.float64).reshape(-1)
+        if derivs.size != 3 * (self.order - 2):
+            raise ValueError(f"derivs needs {3 * (self.order - 2)} values")
+        self._check(self._lib.hb_set_jp(self._h, int(addr), _dptr(pos), float(mass), _dptr(vel),
+                                        float(tlast), _dptr(derivs)), "set_jp")
+
+    def set_jp_records(self, records: np.ndarray, addr0: int = 0):
+        rec = np.ascontiguousarray(records, dtype=np.float64).reshape(-1, self.R)
+        self._check(self._lib.hb_set_jp_records(self._h, int(addr0), rec.shape[0], _dptr(rec)),
+                    "set_jp_records")
+
+    def predict_all(self, tsys: float):
+        self._check(self._lib.hb_predict_all(self._h, float(tsys)), "predict_all")
+
+    def calc_force_on_first_nact(self, nact: int, eps2: float, out: np.ndarray | None = None):
+        if out is None:
+            out = np.empty((max(int(nact), 0), self.F), dtype=np.float64)
+        self._check(self._lib.hb_force_first_nact(self._h, int(nact), float(eps2), _dptr(out)),
+                    "calc_force_on_first_nact")
+        return out
+
+    def calc_potential(self, eps2: float, out: np.ndarray | None = None):
+        if out is None:
+            out = np.empty(self.nbody, dtype=np.float64)
+        self._check(self._lib.hb_potential(self._h, float(eps2), _dptr(out)), "calc_potential")
+        return out
+
+    # -- extras ----------------------------------------------------------------
+    def set_precision(self, precision):
+        self._check(self._lib.hb_set_precision(self._h, _PREC[precision]), "set_precision")
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self._lib.hb_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)),
+                    "set_stream")
+
+    def upload(self):
+        self._check(self._lib.hb_upload(self._h), "upload")
+
+    def predict_all_device(self, tsys: float):
+        self._check(self._lib.hb_predict_all_device(self._h, float(tsys)), "predict_all_device")
+
+    def force_device(self, nact: int, eps2: float):
+        self._check(self._lib.hb_force_device(self._h, int(nact), float(eps2)), "force_device")
+
+    def download_forces(self, nact: int, out: np.ndarray | None = None):
+        if out is None:
+            out = np.empty((int(nact), self.F), dtype=np.float64)
+        self._check(self._lib.hb_download_forces(self._h, int(nact), _dptr(out)), "download_forces")
+        return out
+
+    def synchronize(self):
+        self._check(self._lib.hb_synchronize(self._h), "synchronize")
+
+    def launch_count(self) -> int:
+        return int(self._lib.hb_launch_count(self._h))
+
+    def set_force_shape(self, variant: int = -1, jsplit: int = 0):
+        self._check(self._lib.hb_set_force_shape(self._h, int(variant), int(jsplit)),
+                    "set_force_shape")
+
+    def device_forces_ptr(self) -> int:
+        return int(self._lib.hb_device_forces(self._h) or 0)

@@ -1,0 +1,20 @@
+// hb_force_64.cu -- FP64 force kernel instantiations (orders 4, 6, 8).
+#include "hb_force_table.cuh"
+
+namespace hb {
+
+const ForceVariant *force_variant_64(int order, int v)
+{
+    static const VariantTable<4, false> t4;
+    static const VariantTable<6, false> t6;
+    static const VariantTable<8, false> t8;
+    if (v < 0 || v >= VariantTable<4, false>::count) return nullptr;
+    switch (order) {
+    case 4: return &t4.v[v];
+    case 6: return &t6.v[v];
+    case 8: return &t8.v[v];
+    }
+    return nullptr;
+}
+
+}  // namespace hb

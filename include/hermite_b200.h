@@ -1,0 +1,148 @@
+/*
+ * hermite_b200.h -- C ABI of the B200 (sm_100a) Hermite force calculator.
+ *
+ * This is the boundary that replaces the reference's CUDA force calculator,
+ * the compile-time C++ `struct Gravity` of SRC/hermite{4,6,8}-titan.h that
+ * SRC/hermite{4,6,8}.h select with -DCUDA_TITAN (e.g. SRC/hermite4.h:286-287)
+ * and that the integrator drives (SRC/nbodysystem.h:308,326,565-765).  Each
+ * entry point names the reference member it stands for.  The C++ drop-in that
+ * maps `struct Gravity` onto these calls is hermite_b200/gravity/.
+ *
+ * Plain pointers and sizes only; no CUDA or torch types in the signatures.
+ * Every function returns an int status (HB_OK == 0).  The reference has no
+ * status codes (it prints and aborts through checkCudaErrors,
+ * SRC/cuda_pointer.h:6-10); the C++ drop-in restores that behaviour.
+ *
+ * Data formats (doubles, little-endian host order):
+ *   j-particle record, 8 + 3*(order-2) words (14 / 20 / 26):
+ *     pos[3] mass vel[3] tlast acc[3] jrk[3] [snp[3] crk[3]] [d4a[3] d5a[3]]
+ *     (the field order of the reference's GParticle, SRC/hermite4-titan.h:20-27,
+ *      SRC/hermite6-titan.h:20-29, SRC/hermite8-titan.h:20-31)
+ *   force record, 3*(order/2) words (6 / 9 / 12):
+ *     acc[3] jrk[3] [snp[3]] [crk[3]]
+ *     (the reference's `struct Force`, SRC/hermite4.h:4-14, SRC/hermite6.h:4-17,
+ *      SRC/hermite8.h:8-24)
+ *
+ * Threading: hb_set_jp / hb_set_jp_records may be called concurrently from
+ * several host threads on distinct slots (the integrator does so from OpenMP
+ * workers, SRC/nbodysystem.h:753-756).  Every other call on one context must
+ * come from one thread at a time.
+ */
+#ifndef HERMITE_B200_H
+#define HERMITE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hb_ctx hb_ctx;
+
+enum hb_status {
+    HB_OK = 0,
+    HB_ERR_INVALID = 1,        /* an argument is out of range              */
+    HB_ERR_CUDA = 2,           /* a CUDA runtime call failed               */
+    HB_ERR_ALLOC = 3,          /* device or pinned host allocation failed  */
+    HB_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait gave up       */
+    HB_ERR_NO_DEVICE = 5,      /* no CUDA device, or not an sm_100 device  */
+    HB_ERR_STATE = 6           /* call out of order (e.g. force before any
+                                  predict_all)                            */
+};
+
+enum hb_precision {
+    HB_FP64 = 0,  /* plain FP64 interaction and accumulation (the judge)     */
+    HB_MIXED = 1  /* FP64 predictor; hi/lo FP32 relative positions; FP32
+                     interaction; FP32 partial sums flushed into FP64
+                     accumulators; FP64 crackle accumulation at 8th order    */
+};
+
+/* Gravity(int nbody) -- SRC/hermite4-titan.h:49-57 (also 6th/8th).
+ * order is 4, 6 or 8; 1 <= nbody <= 1<<24.  Allocates device buffers and
+ * pinned host mirrors once; nothing is allocated per call afterwards. */
+int hb_create(int order, int nbody, int precision, hb_ctx **out);
+
+/* ~Gravity() -- SRC/hermite4-titan.h:58-63.  NULL is accepted. */
+int hb_destroy(hb_ctx *ctx);
+
+/* Gravity::set_jp(int addr, const Particle p) -- SRC/hermite4-titan.h:70-78,
+ * SRC/hermite6-titan.h:70-97, SRC/hermite8-titan.h:77-112.
+ * Writes slot `addr` of the pinned host mirror only.  `derivs` holds
+ * 3*(order-2) doubles: acc jrk [snp crk] [d4a d5a]. */
+int hb_set_jp(hb_ctx *ctx, int addr, const double pos[3], double mass,
+              const double vel[3], double tlast, const double *derivs);
+
+/* Bulk form of set_jp: `count` consecutive records starting at slot addr0. */
+int hb_set_jp_records(hb_ctx *ctx, int addr0, int count, const double *records);
+
+/* Gravity::predict_all(double tsys) -- SRC/hermite4-titan.cu:102-116.
+ * Uploads the slots changed since the last upload (the reference uploads the
+ * first `njpsend` = previous nact slots, SRC/hermite4-titan.cu:103,411; this
+ * also covers any other slot passed to set_jp), then predicts every slot to
+ * tsys from its own tlast.  Asynchronous: returns once work is queued. */
+int hb_predict_all(hb_ctx *ctx, double tsys);
+
+/* Gravity::calc_force_on_first_nact(int nact, double eps2, Force force[]) --
+ * SRC/hermite4-titan.cu:362-412, SRC/hermite6-titan.cu:362-405,
+ * SRC/hermite8-titan.cu:428-473.  Force on slots [0,nact) from all slots,
+ * self pair included (exactly zero for eps2 > 0).  Writes nact force records
+ * to force_out and returns when they are there.  0 <= nact <= nbody. */
+int hb_force_first_nact(hb_ctx *ctx, int nact, double eps2, double *force_out);
+
+/* Gravity::calc_potential(double eps2, double potbuf[]) --
+ * SRC/pot-titan.hu:131-171.  phi_i = -sum_{j != i} m_j / sqrt(r^2 + eps2)
+ * on the un-predicted positions of the host mirror (pending set_jp slots are
+ * uploaded first).  Writes nbody doubles to pot_out. */
+int hb_potential(hb_ctx *ctx, double eps2, double *pot_out);
+
+/* Switch between HB_FP64 and HB_MIXED.  Takes effect at the next
+ * predict_all (the predicted layout differs). */
+int hb_set_precision(hb_ctx *ctx, int precision);
+int hb_get_precision(const hb_ctx *ctx);
+
+/* Last error message of this context ("" if none); static text for NULL. */
+const char *hb_last_error(const hb_ctx *ctx);
+const char *hb_status_string(int status);
+
+/* ---- device-resident forms (no host<->device copies) -------------------
+ * For callers that keep inputs and results in HBM, and for timing the
+ * kernels alone.  None of these has a reference counterpart; they split
+ * predict_all / calc_force_on_first_nact at the copy boundaries. */
+
+/* Run all later work of this context on the given cudaStream_t (NULL restores
+ * the context's own stream). */
+int hb_set_stream(hb_ctx *ctx, void *cuda_stream);
+/* Upload pending set_jp slots now (the copy part of predict_all). */
+int hb_upload(hb_ctx *ctx);
+/* The kernel part of predict_all: predict every slot, no upload. */
+int hb_predict_all_device(hb_ctx *ctx, double tsys);
+/* The kernel part of calc_force_on_first_nact: results stay in HBM
+ * (hb_device_forces), nothing is copied back, no synchronisation. */
+int hb_force_device(hb_ctx *ctx, int nact, double eps2);
+/* Copy nact force records of the last hb_force_device to the host. */
+int hb_download_forces(hb_ctx *ctx, int nact, double *force_out);
+/* Device address of the force records (nbody x 3*(order/2) doubles). */
+const double *hb_device_forces(const hb_ctx *ctx);
+/* Wait for the context's queued work; reports device-side wait timeouts. */
+int hb_synchronize(hb_ctx *ctx);
+/* Number of kernels this context has launched so far. */
+long long hb_launch_count(const hb_ctx *ctx);
+
+/* Launch shape of the force kernel, picked per (order, precision, nbody,
+ * nact) by the built-in tuning table unless overridden here.  variant
+ * indexes the compiled kernel variants (see hb_force_variant_count);
+ * jsplit is the number of j-slices (CTAs per i-tile); 0 means "auto". */
+int hb_set_force_shape(hb_ctx *ctx, int variant, int jsplit);
+int hb_force_variant_count(int order, int precision);
+/* Describe a variant: threads per CTA, i per thread, warps splitting j. */
+int hb_force_variant_info(int order, int precision, int variant,
+                          int *threads, int *i_per_thread, int *j_warps);
+
+/* Measured peak of the FP32 (precision = HB_MIXED) or FP64 (HB_FP64) FMA
+ * pipe on the current device, in GFLOP/s (2 flops per FMA), from a
+ * register-resident FMA-chain kernel.  A roofline denominator for the force
+ * kernels; no reference counterpart. */
+int hb_measure_fma_peak(int precision, double *gflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HERMITE_B200_H */
