@@ -1,0 +1,466 @@
+"""Benchmark of the Hermite force hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Headline workload (one "step" = one block step with every particle active,
+the reference's "Init N square" step, SRC/nbodysystem.h:582-594):
+    plain FP64 4th order, Plummer N = 65536, equal masses, Henon units,
+    eps = 1/1024: predict_all over all N, then the force on all N (N^2
+    interactions, self pair included, 60 flops each by the reference's
+    convention, SRC/hermite4.h:19).
+  value  -- Gint/s with inputs resident in HBM (predictor + force kernels),
+            L2 flushed before every timed step.
+  e2e    -- the same step through the C ABI with host buffers: set_jp of
+            all N records, predict_all (host->device upload), force into host
+            memory (device->host), all inside the timed region.
+Extra keys: the roofline of the force kernel against the FP64 FMA peak
+measured in the same run; the reference's own AVX2 CPU Gravity (built from
+its sources into oracle/_ref/) on a bounded sample as cpu_baseline; the
+mixed-precision vs FP64 6th-order kernels at N = 262144 with their force
+errors (configs[2]-style); block-step latency through the C ABI at several
+nact.
+
+--impl reference times the reference's AVX2 Gravity (set_jp, predict_all,
+calc_force_on_first_nact) on this host's cores, on a bounded sample of the
+same workload.  Under torchrun only rank 0 runs it.
+--gpus N > 1 runs N independent replicas (the path does not shard across
+GPUs in the reference; one process per GPU), timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gint/s & block-step time, mixed-prec vs FP64 kernel, 1 B200, at stated force/energy err"
+UNIT = "Gint/s"
+ORDER, N, EPS = 4, 65536, 1.0 / 1024
+FLOPS = {4: 60, 6: 97, 8: 144}
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload_config(extra=None):
+    cfg = {"workload": "Plummer N=65536 equal-mass Henon units, eps=1/1024, 4th-order Hermite, "
+                       "plain FP64; one step = predict_all + force on all N (full block step)",
+           "order": ORDER, "nbody": N, "nact": N, "eps": EPS, "precision": "fp64",
+           "flops_per_interaction": FLOPS[ORDER], "l2": "flushed (256 MiB write) before each step",
+           "parallelism": "replicas"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def plummer_records(order, n, seed=0):
+    from hermite_b200.ic import plummer, records
+    return records(plummer(n, seed), order)
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+def host_threads() -> int:
+    """CPUs this process may run on (libgomp's default team size)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_force_rate(order, n, nact, reps, threads, rec=None):
+    """The reference's AVX2 Gravity (oracle/_ref) on this host: Gint/s."""
+    from oracle import RefGravity
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    if rec is None:
+        rec = plummer_records(order, n)
+    g = RefGravity(order, n, "avx")
+    eps2 = EPS * EPS
+    g.set_jp_all(rec)
+    g.predict_all(0.0)
+    g.force(nact, eps2)                     # warm-up
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        g.set_jp_all(rec)
+        g.predict_all(0.0)
+        g.force(nact, eps2)
+        times.append(time.perf_counter() - t0)
+    g.close()
+    return nact * n / (sum(times) / len(times)) * 1e-9, times
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = host_threads()
+    from oracle import ref_available
+    if not ref_available("avx", ORDER):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libref_avx4.so not built (needs the reference sources)"}))
+        return
+    nact = 8192                              # bounded sample: 8192 i x 65536 j per step
+    rec = plummer_records(ORDER, N)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import RefGravity
+    g = RefGravity(ORDER, N, "avx")
+    eps2 = EPS * EPS
+    for _ in range(args.warmup):
+        g.set_jp_all(rec)
+        g.predict_all(0.0)
+        g.force(nact, eps2)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        g.set_jp_all(rec)
+        g.predict_all(0.0)
+        g.force(nact, eps2)
+    dt = time.perf_counter() - t0
+    g.close()
+    value = nact * N * args.steps / dt * 1e-9
+    sample = f"force on the first {nact} of {N} particles from all {N} per step"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config({"impl": "reference AVX2 Gravity "
+                                                        "(SRC/hermite4-avx.h) on host cores"}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---------------------------------------------------------------------------
+def traffic_from_profiles():
+    """dram bytes per force-kernel launch from the committed ncu summary."""
+    p = ROOT / "profiles" / "force_fp64_o4_n65536.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args):
+    import torch
+    from hermite_b200 import Gravity, measure_fma_peak
+
+    world, rank, local = dist_setup(args)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    rec = plummer_records(ORDER, N, seed=rank)
+    eps2 = EPS * EPS
+    nint = float(N) * N
+
+    with torch.cuda.stream(stream):
+        g = Gravity(ORDER, N, "fp64")
+        g.set_stream(stream.cuda_stream)
+        g.set_jp_records(rec)
+        g.upload()
+        for _ in range(args.warmup):
+            g.predict_all_device(0.0)
+            g.force_device(N, eps2)
+        stream.synchronize()
+
+        # ---- device-resident timed region ----
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+               torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        l0 = g.launch_count()
+        dist_barrier(world)
+        torch.cuda.synchronize(dev)
+        with ClockSampler(local) as clk:
+            for k in range(args.steps):
+                flush.zero_()
+                e0, e1, e2 = ev[k]
+                e0.record(stream)
+                g.predict_all_device(1e-3 * (k + 1))
+                e1.record(stream)
+                g.force_device(N, eps2)
+                e2.record(stream)
+            torch.cuda.synchronize(dev)
+        dist_barrier(world)
+        launches = g.launch_count() - l0
+        step_ms = [a.elapsed_time(c) for a, b, c in ev]
+        force_ms = [b.elapsed_time(c) for a, b, c in ev]
+        pred_ms = [a.elapsed_time(b) for a, b, c in ev]
+        total_ms = dist_max(sum(step_ms), world)
+        value = nint * args.steps * world / (total_ms * 1e-3) * 1e-9
+
+        # ---- end to end through the C ABI with host buffers ----
+        out = np.empty((N, 6))
+        g.set_stream(None)
+        for _ in range(2):
+            g.set_jp_records(rec)
+            g.predict_all(0.0)
+            g.calc_force_on_first_nact(N, eps2, out)
+        dist_barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            g.set_jp_records(rec)
+            g.predict_all(0.0)
+            g.calc_force_on_first_nact(N, eps2, out)
+        e2e_s = dist_max(time.perf_counter() - t0, world)
+        e2e = nint * args.steps * world / e2e_s * 1e-9
+
+        # ---- block-step latency through the C ABI (predict_all + force) ----
+        block_us = {}
+        for nact in (1, 32, 1024, 8192, N):
+            buf = np.empty((nact, 6))
+            for _ in range(3):
+                g.predict_all(0.0)
+                g.calc_force_on_first_nact(nact, eps2, buf)
+            reps = 50 if nact < N else 5
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                g.set_jp_records(rec[:nact])
+                g.predict_all(0.0)
+                g.calc_force_on_first_nact(nact, eps2, buf)
+            block_us[str(nact)] = (time.perf_counter() - t0) / reps * 1e6
+        g.close()
+
+    fp64_peak = measure_fma_peak(0)      # GFLOP/s, same device, same run
+    fp32_peak = measure_fma_peak(2)
+    force_avg_ms = sum(force_ms) / len(force_ms)
+    achieved = nint * FLOPS[ORDER] / (force_avg_ms * 1e-3) * 1e-12
+    traffic = traffic_from_profiles()
+
+    mixed = mixed_vs_fp64(dev, stream) if not args.skip_mixed else None
+
+    if rank != 0:
+        dist_barrier(world)
+        return
+    cpu = None
+    if not args.skip_cpu:
+        try:
+            from oracle import ref_available
+            if ref_available("avx", ORDER):
+                threads = host_threads()
+                nact = 8192
+                rate, times = reference_force_rate(ORDER, N, nact, 3, threads, rec)
+                cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                       "sample": f"reference AVX2 Gravity (SRC/hermite4-avx.h, built from source): "
+                                 f"set_jp + predict_all + force on the first {nact} of {N} "
+                                 f"particles, 3 reps, {sum(times):.1f} s total"}
+        except Exception as e:          # the baseline is reported, not required
+            cpu = {"value": None, "unit": UNIT, "cores": host_threads(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(),
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": N * 14 * 8,
+                "d2h_bytes_per_step": N * 6 * 8},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak * 1e-3,
+                     "unit": "TFLOP/s", "frac": achieved / (fp64_peak * 1e-3), "traffic": traffic,
+                     "kernel": "hb::force_kernel<4, FP64>",
+                     "peak_source": "FP64 FMA-chain kernel measured in this run "
+                                    "(hb_measure_fma_peak); MEASURED_PEAKS.json has no FP64 figure",
+                     "achieved_basis": f"N^2 x {FLOPS[ORDER]} flops per launch / mean CUDA-event "
+                                       "duration of the force launch"},
+        "kernel_ms": {"predict": sum(pred_ms) / len(pred_ms), "force": force_avg_ms},
+        "fp32_peak_tflops": fp32_peak * 1e-3,
+        "block_step_us": {"order": ORDER, "nbody": N, "precision": "fp64",
+                          "through": "set_jp(nact) + predict_all + calc_force_on_first_nact",
+                          "us": block_us},
+        "mixed_vs_fp64": mixed,
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    dist_barrier(world)
+
+
+def mixed_vs_fp64(dev, stream):
+    """6th order, Plummer N = 262144, eps = 1/4096: full N^2 force in the
+    mixed-precision and FP64 kernels, and the per-particle relative force
+    error of the mixed kernel against the FP64 kernel on a 4096-particle
+    sample."""
+    import torch
+    from hermite_b200 import Gravity
+    order, n, eps2, reps = 6, 262144, (1.0 / 4096) ** 2, 2
+    rec = plummer_records(order, n, seed=7)
+    res = {"order": order, "nbody": n, "eps": 1.0 / 4096, "flops_per_interaction": FLOPS[order]}
+    forces = {}
+    for prec in ("fp64", "mixed"):
+        with torch.cuda.stream(stream):
+            g = Gravity(order, n, prec)
+            g.set_stream(stream.cuda_stream)
+            g.set_jp_records(rec)
+            g.upload()
+            g.predict_all_device(0.0)
+            g.force_device(n, eps2)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                g.force_device(n, eps2)
+            e1.record(stream)
+            stream.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            g.set_stream(None)
+            forces[prec] = g.calc_force_on_first_nact(4096, eps2)
+            g.close()
+        rate = float(n) * n / (ms * 1e-3) * 1e-9
+        res[prec] = {"gint_s": rate, "tflops": rate * FLOPS[order] * 1e-3, "force_ms": ms}
+    res["speedup"] = res["mixed"]["gint_s"] / res["fp64"]["gint_s"]
+    a, b = forces["mixed"].reshape(4096, 3, 3), forces["fp64"].reshape(4096, 3, 3)
+    err = np.linalg.norm(a - b, axis=2) / np.linalg.norm(b, axis=2)
+    res["rel_err_vs_fp64"] = {name: {"max": float(err[:, k].max()), "median": float(np.median(err[:, k]))}
+                              for k, name in enumerate(("acc", "jrk", "snp"))}
+    return res
+
+
+def run_profile_case(case: str):
+    """One small predict + two force launches, for ncu captures:
+    fp64_o4 = the headline kernel (4th order FP64, N = 65536, all active);
+    mixed_o6 = 6th-order mixed precision, N = 65536, all active."""
+    from hermite_b200 import Gravity
+    order, prec = {"fp64_o4": (4, "fp64"), "mixed_o6": (6, "mixed"),
+                   "fp64_o6": (6, "fp64"), "mixed_o8": (8, "mixed")}[case]
+    g = Gravity(order, N, prec)
+    g.set_jp_records(plummer_records(order, N))
+    g.predict_all(0.0)
+    for _ in range(2):
+        g.force_device(N, EPS * EPS)
+    g.synchronize()
+    g.close()
+    print(f"profile case {case} done")
+
+
+def main():
+    ap = argparse.ArgumentParser(description="Hermite force hot-path benchmark")
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
+    ap.add_argument("--skip-mixed", action="store_true", help="omit the mixed-vs-FP64 leg")
+    ap.add_argument("--profile", choices=("fp64_o4", "mixed_o6", "fp64_o6", "mixed_o8"),
+                    help="run one small case for an ncu capture and exit")
+    args = ap.parse_args()
+    if args.profile:
+        run_profile_case(args.profile)
+        return
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch.distributed as dist
+        if dist.is_initialized():
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
