@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = (
     "hb_last_error", "hb_status_string", "hb_set_stream", "hb_upload",
     "hb_predict_all_device", "hb_force_device", "hb_download_forces", "hb_device_forces",
     "hb_synchronize", "hb_launch_count", "hb_set_force_shape", "hb_force_variant_count",
-    "hb_force_variant_info", "hb_measure_fma_peak",
+    "hb_force_variant_info", "hb_measure_fma_peak", "hb_force_predicted_noalloc",
 )
 
 
@@ -102,6 +102,7 @@ def load_library() -> ctypes.CDLL:
         "hb_force_variant_info": (I, [I, I, I, ctypes.POINTER(I), ctypes.POINTER(I),
                                       ctypes.POINTER(I)]),
         "hb_measure_fma_peak": (I, [I, dp]),
+        "hb_force_predicted_noalloc": (I, [I, I, P, I, I, D, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -30,7 +30,8 @@ INCLUDE = ROOT / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
               "--expt-relaxed-constexpr", "-I", str(INCLUDE), "-I", str(CSRC)]
-SOURCES = ["hb_capi.cu", "hb_predict_pot.cu", "hb_force_64.cu", "hb_force_mixed.cu"]
+SOURCES = ["hb_capi.cu", "hb_predict_pot.cu", "hb_force_64.cu", "hb_force_mixed.cu",
+           "hb_noalloc.cu"]
 HEADERS = ["hb_common.cuh", "hb_math.cuh", "hb_force.cuh", "hb_force_table.cuh",
            "hb_internal.h"]
 

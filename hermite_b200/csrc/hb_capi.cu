@@ -214,6 +214,7 @@ const char *hb_status_string(int s)
     case HB_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
     case HB_ERR_NO_DEVICE: return "no sm_100 CUDA device";
     case HB_ERR_STATE: return "call out of order";
+    case HB_ERR_TOO_LARGE: return "size exceeds a fixed capacity";
     }
     return "unknown status";
 }

@@ -44,8 +44,10 @@ enum hb_status {
     HB_ERR_ALLOC = 3,          /* device or pinned host allocation failed  */
     HB_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait gave up       */
     HB_ERR_NO_DEVICE = 5,      /* no CUDA device, or not an sm_100 device  */
-    HB_ERR_STATE = 6           /* call out of order (e.g. force before any
+    HB_ERR_STATE = 6,          /* call out of order (e.g. force before any
                                   predict_all)                            */
+    HB_ERR_TOO_LARGE = 7       /* a size exceeds a fixed capacity (see
+                                  hb_force_predicted_noalloc)             */
 };
 
 enum hb_precision {
@@ -141,6 +143,39 @@ int hb_force_variant_info(int order, int precision, int variant,
  * register-resident FMA-chain kernel.  A roofline denominator for the force
  * kernels; no reference counterpart. */
 int hb_measure_fma_peak(int precision, double *gflops);
+
+/* ---- allocation-free force ---------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code inside a host framework that owns every device allocation through its
+ * own pool, code that enqueues work while a stream is being captured into a
+ * CUDA graph (cudaMalloc is not allowed there), and fixed-budget jobs on a
+ * shared GPU that must not grow their footprint after start-up.  hb_create
+ * allocates, so such callers use this context-free entry point instead; it
+ * allocates nothing.
+ *
+ * Computes the force on slots [0,nact) from all nslots slots, like
+ * hb_force_device, from predicted j-particles the caller already holds in
+ * device memory, in the library's predicted layout ("AoSoA32": chunks of 32
+ * slots, each chunk one 32-wide vector per component;
+ *   HB_FP64:  x y z m vx vy vz [ax ay az] [jx jy jz]              (double)
+ *   HB_MIXED: xh yh zh xl yl zl m vx vy vz [ax ay az] [jx jy jz]   (float,
+ *             position = hi + lo)
+ * with unused slots given zero mass at distinct far-away positions).  Writes
+ * nact force records (3*(order/2) doubles each) to the device array `force`.
+ * Asynchronous on `stream` (a cudaStream_t; NULL = the default stream).
+ *
+ * Limits: nslots a multiple of 256 and at most 1<<20 (HB_ERR_TOO_LARGE
+ * beyond); larger nact get fewer j-slices, never a larger buffer.
+ * Scratch: one file-scope device array of 4.125 MiB (4 MiB of j-slice
+ * partial sums, 128 KiB of arrival counters) that every GPU loading the
+ * library holds until the process exits.  The first call on each device looks
+ * up that array's device address; make that first call before any stream
+ * capture.  Every call shares the array and clears the counters it uses on
+ * its stream first; calls that overlap on the GPU (on different streams or
+ * devices sharing a context) race on it and must be serialised by the caller.
+ * A device-side wait that gives up is not reported by this entry point. */
+int hb_force_predicted_noalloc(int order, int precision, const void *pred, int nslots,
+                               int nact, double eps2, double *force, void *stream);
 
 #ifdef __cplusplus
 }
