@@ -332,6 +332,9 @@ def run_ours(args):
     traffic = traffic_from_profiles()
 
     mixed = mixed_vs_fp64(dev, stream) if not args.skip_mixed else None
+    integ = device_integrator_leg() if not args.skip_integrator else None
+    ref_gpu = reference_gpu_leg() if not args.skip_integrator else None
+    ens = ensemble_leg() if not args.skip_integrator else None
 
     if rank != 0:
         dist_barrier(world)
@@ -373,6 +376,9 @@ def run_ours(args):
                           "through": "set_jp(nact) + predict_all + calc_force_on_first_nact",
                           "us": block_us},
         "mixed_vs_fp64": mixed,
+        "device_integrator": integ,
+        "reference_gpu_recompiled": ref_gpu,
+        "ensemble": ens,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
@@ -436,6 +442,91 @@ def run_profile_case(case: str):
     print(f"profile case {case} done")
 
 
+def device_integrator_leg(configs=("c1", "c2")):
+    """Block-step time of the device-resident integrator (corrector and
+    scheduler on the GPU, 32 block steps per CUDA-graph replay) on the
+    plain-FP64 configurations c1 and c2 of hermite_b200.run_app (eta = 0.01:
+    the mixed path is not used at such small eta, where FP32 force noise
+    collapses the Aarseth steps): wall time per block step, particle steps x
+    N / time, and the energy error."""
+    from hermite_b200 import Gravity
+    from hermite_b200.ic import plummer, records
+    from hermite_b200.run_app import CONFIGS
+    out = {}
+    for name in configs:
+        cfg = dict(CONFIGS[name])
+        if name == "c2":
+            cfg["tend"] = 1.0 / 64          # a window: the full run is ~1e7 block steps
+        order, n = cfg["order"], cfg["n"]
+        eps2 = cfg["eps"] ** 2
+        for prec in ("fp64",):
+            with Gravity(order, n, prec) as g:
+                g.set_jp_records(records(plummer(n, 0), order))
+                g.integrator_init(0.0, eps2, cfg["eta"], cfg["eta_s"], 1.0 / cfg["dtmaxinv"])
+                ke0, pe0 = g.energy(eps2)
+                t0 = time.perf_counter()
+                g.integrator_run(cfg["tend"], max_block_steps=2_000_000)
+                wall = time.perf_counter() - t0
+                ps, bs, t = g.integrator_stats()
+                ke, pe = g.energy(eps2)
+            e0 = ke0 + pe0
+            out[f"{name}_{prec}"] = {
+                "order": order, "n": n, "tend": cfg["tend"], "block_steps": bs,
+                "particle_steps": ps, "nact_mean": ps / max(bs, 1), "wall_s": wall,
+                "us_per_block": wall / max(bs, 1) * 1e6, "gint_s": ps * n / wall * 1e-9,
+                "de_global": (e0 - (ke + pe)) / e0}
+    return out
+
+
+def ensemble_leg(nclusters=256, tend=1.0 / 16):
+    """Batched ensemble (configs[4]-style): clusters with seeds 0..255, N
+    log-uniform in [1024, 32768], power-law masses (slope -2.35 on [0.1, 100],
+    total 1), eps = 4/N each, 6th order mixed precision, eta = 0.1
+    (eta_s = eta/5), dtmax = 1/16, integrated by one device-resident loop;
+    window t = 0..tend.  Interactions = sum over block steps and clusters of
+    nact_c * N_c."""
+    from hermite_b200 import Ensemble
+    from hermite_b200.ic import plummer, power_law_masses, records
+    rng = np.random.default_rng(2024)
+    sizes = [int(round(np.exp(rng.uniform(np.log(1024), np.log(32768))))) for _ in range(nclusters)]
+    out = {"clusters": nclusters, "n_total": int(sum(sizes)), "order": 6, "precision": "mixed",
+           "eta": 0.1, "eta_s": 0.02, "dtmax": 1.0 / 16, "tend": tend}
+    with Ensemble(6, sizes, "mixed") as ens:
+        for c, n in enumerate(sizes):
+            r = np.random.default_rng(c)
+            snap = plummer(n, seed=c, masses=power_law_masses(n, r))
+            ens.set_cluster(c, records(snap, 6), (4.0 / n) ** 2)
+        ens.init(0.0, 0.1, 0.02, 1.0 / 16)
+        ke0, pe0 = ens.energy()
+        t0 = time.perf_counter()
+        ens.run(tend, max_block_steps=400_000)
+        wall = time.perf_counter() - t0
+        ps, bs, t, inter = ens.stats()
+        ke1, pe1 = ens.energy()
+    de = (ke0 + pe0 - ke1 - pe1) / (ke0 + pe0)
+    out.update({"wall_s": wall, "block_steps": bs, "particle_steps": ps,
+                "us_per_block": wall / max(bs, 1) * 1e6, "gint_s": inter / wall * 1e-9,
+                "de_global_max_abs": float(np.max(np.abs(de))),
+                "de_global_median_abs": float(np.median(np.abs(de)))})
+    return out
+
+
+def reference_gpu_leg():
+    """The reference's own FP64 CUDA force path (SRC/hermite4-titan.cu, written
+    for sm_35) recompiled unmodified for sm_100a (oracle/_ref/titan-4), on the
+    headline workload: its own "## Init N square" report of one full N^2
+    force evaluation at N = 65536, and its app-level block-step rate over a
+    short window of configuration c2."""
+    from hermite_b200.run_app import APP, run
+    if not Path(str(APP["ref-gpu"]).format(order=4)).exists():
+        return None
+    r = run("c2", "ref-gpu", tend=1.0 / 512)
+    return {"binary": "oracle/_ref/titan-4 (reference SRC/hermite4-titan.cu, sm_100a)",
+            "init_n2_gint_s": r["init_n2_gflops"] / FLOPS[ORDER] if r["init_n2_gflops"] else None,
+            "app_us_per_block": r.get("us_per_block"), "app_gint_s": r.get("app_gint_s"),
+            "window": "c2 (N=65536, eps=1/1024, eta=0.01) t = 0..1/512"}
+
+
 def main():
     ap = argparse.ArgumentParser(description="Hermite force hot-path benchmark")
     ap.add_argument("--gpus", type=int, default=1)
@@ -444,6 +535,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
     ap.add_argument("--skip-mixed", action="store_true", help="omit the mixed-vs-FP64 leg")
+    ap.add_argument("--skip-integrator", action="store_true",
+                    help="omit the device-integrator block-step leg")
     ap.add_argument("--profile", choices=("fp64_o4", "mixed_o6", "fp64_o6", "mixed_o8"),
                     help="run one small case for an ncu capture and exit")
     args = ap.parse_args()

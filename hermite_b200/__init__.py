@@ -26,7 +26,7 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ["Gravity", "HermiteError", "record_words", "force_words", "FP64", "MIXED",
+__all__ = ["Gravity", "Ensemble", "HermiteError", "record_words", "force_words", "FP64", "MIXED",
            "library_path", "load_library", "measure_fma_peak", "EXPORTED_SYMBOLS"]
 
 FP64 = 0
@@ -45,6 +45,10 @@ EXPORTED_SYMBOLS = (
     "hb_predict_all_device", "hb_force_device", "hb_download_forces", "hb_device_forces",
     "hb_synchronize", "hb_launch_count", "hb_set_force_shape", "hb_force_variant_count",
     "hb_force_variant_info", "hb_measure_fma_peak", "hb_force_predicted_noalloc",
+    "hb_integrator_init", "hb_integrator_run", "hb_integrator_stats", "hb_energy",
+    "hb_get_records", "hb_ens_create", "hb_ens_destroy", "hb_ens_last_error",
+    "hb_ens_set_cluster", "hb_ens_get_cluster", "hb_ens_cluster_offset", "hb_ens_init",
+    "hb_ens_run", "hb_ens_stats", "hb_ens_energy",
 )
 
 
@@ -103,6 +107,23 @@ def load_library() -> ctypes.CDLL:
                                       ctypes.POINTER(I)]),
         "hb_measure_fma_peak": (I, [I, dp]),
         "hb_force_predicted_noalloc": (I, [I, I, P, I, I, D, P, P]),
+        "hb_integrator_init": (I, [P, D, D, D, D, D]),
+        "hb_integrator_run": (I, [P, D, ctypes.c_longlong]),
+        "hb_integrator_stats": (I, [P, ctypes.POINTER(ctypes.c_longlong),
+                                    ctypes.POINTER(ctypes.c_longlong), dp]),
+        "hb_energy": (I, [P, D, dp, dp]),
+        "hb_get_records": (I, [P, I, I, dp, dp]),
+        "hb_ens_create": (I, [I, I, ctypes.POINTER(I), I, ctypes.POINTER(P)]),
+        "hb_ens_destroy": (I, [P]),
+        "hb_ens_last_error": (ctypes.c_char_p, [P]),
+        "hb_ens_set_cluster": (I, [P, I, dp, D]),
+        "hb_ens_get_cluster": (I, [P, I, dp, dp]),
+        "hb_ens_cluster_offset": (I, [P, I]),
+        "hb_ens_init": (I, [P, D, D, D, D]),
+        "hb_ens_run": (I, [P, D, ctypes.c_longlong]),
+        "hb_ens_stats": (I, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                             dp, dp]),
+        "hb_ens_energy": (I, [P, dp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -232,3 +253,106 @@ class Gravity:
 
     def device_forces_ptr(self) -> int:
         return int(self._lib.hb_device_forces(self._h) or 0)
+
+    # -- device-resident integration (corrector + block-step scheduler) --------
+    def integrator_init(self, tsys: float, eps2: float, eta: float, eta_s: float, dtmax: float):
+        self._check(self._lib.hb_integrator_init(self._h, float(tsys), float(eps2), float(eta),
+                                                 float(eta_s), float(dtmax)), "integrator_init")
+
+    def integrator_run(self, tend: float, max_block_steps: int = 0):
+        self._check(self._lib.hb_integrator_run(self._h, float(tend), int(max_block_steps)),
+                     "integrator_run")
+
+    def integrator_stats(self):
+        ps, bs, t = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
+        self._check(self._lib.hb_integrator_stats(self._h, ctypes.byref(ps), ctypes.byref(bs),
+                                                  ctypes.byref(t)), "integrator_stats")
+        return ps.value, bs.value, t.value
+
+    def energy(self, eps2: float):
+        ke, pe = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.hb_energy(self._h, float(eps2), ctypes.byref(ke), ctypes.byref(pe)),
+                    "energy")
+        return ke.value, pe.value
+
+    def get_records(self, addr0: int = 0, count: int | None = None, with_dt: bool = False):
+        count = self.nbody - addr0 if count is None else int(count)
+        rec = np.empty((count, self.R))
+        dt = np.empty(count) if with_dt else None
+        self._check(self._lib.hb_get_records(self._h, int(addr0), count, _dptr(rec),
+                                             _dptr(dt) if with_dt else None), "get_records")
+        return (rec, dt) if with_dt else rec
+
+
+class Ensemble:
+    """Independent clusters integrated together on the device (batched
+    block steps; each particle interacts only with its own cluster)."""
+
+    def __init__(self, order: int, sizes, precision="mixed"):
+        self._lib = load_library()
+        self.order = int(order)
+        self.sizes = [int(n) for n in sizes]
+        self.R, self.F = record_words(self.order), force_words(self.order)
+        arr = (ctypes.c_int * len(self.sizes))(*self.sizes)
+        h = ctypes.c_void_p()
+        st = self._lib.hb_ens_create(self.order, len(self.sizes), arr, _PREC[precision],
+                                     ctypes.byref(h))
+        if st != 0:
+            raise HermiteError(st, "hb_ens_create: " + self._lib.hb_status_string(st).decode())
+        self._h = h
+
+    def _check(self, st, what):
+        if st != 0:
+            msg = self._lib.hb_ens_last_error(self._h).decode() or self._lib.hb_status_string(st).decode()
+            raise HermiteError(st, f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hb_ens_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_cluster(self, c: int, records: np.ndarray, eps2: float):
+        rec = np.ascontiguousarray(records, dtype=np.float64).reshape(-1, self.R)
+        if rec.shape[0] != self.sizes[c]:
+            raise ValueError(f"cluster {c} has {self.sizes[c]} particles")
+        self._check(self._lib.hb_ens_set_cluster(self._h, int(c), _dptr(rec), float(eps2)),
+                    "set_cluster")
+
+    def get_cluster(self, c: int, with_dt: bool = False):
+        rec = np.empty((self.sizes[c], self.R))
+        dt = np.empty(self.sizes[c]) if with_dt else None
+        self._check(self._lib.hb_ens_get_cluster(self._h, int(c), _dptr(rec),
+                                                 _dptr(dt) if with_dt else None), "get_cluster")
+        return (rec, dt) if with_dt else rec
+
+    def init(self, tsys: float, eta: float, eta_s: float, dtmax: float):
+        self._check(self._lib.hb_ens_init(self._h, float(tsys), float(eta), float(eta_s),
+                                          float(dtmax)), "init")
+
+    def run(self, tend: float, max_block_steps: int = 0):
+        self._check(self._lib.hb_ens_run(self._h, float(tend), int(max_block_steps)), "run")
+
+    def stats(self):
+        ps, bs = ctypes.c_longlong(), ctypes.c_longlong()
+        t, inter = ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.hb_ens_stats(self._h, ctypes.byref(ps), ctypes.byref(bs),
+                                           ctypes.byref(t), ctypes.byref(inter)), "stats")
+        return ps.value, bs.value, t.value, inter.value
+
+    def energy(self):
+        ke = np.empty(len(self.sizes))
+        pe = np.empty(len(self.sizes))
+        self._check(self._lib.hb_ens_energy(self._h, _dptr(ke), _dptr(pe)), "energy")
+        return ke, pe

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -17,7 +18,7 @@ namespace hb {
 const ForceVariant *force_variant_64(int order, int v);
 const ForceVariant *force_variant_mixed(int order, int v);
 
-int force_variant_count(int order, bool) { return (order == 4 || order == 6 || order == 8) ? 5 : 0; }
+int force_variant_count(int order, bool) { return (order == 4 || order == 6 || order == 8) ? 18 : 0; }
 
 const ForceVariant *force_variant(int order, bool mixed, int v)
 {
@@ -29,7 +30,7 @@ using namespace hb;
 
 namespace {
 constexpr int kMaxBody = 1 << 24;
-constexpr int kNumVariants = 5;
+constexpr int kNumVariants = 18;
 
 int rec_words(int order) { return 8 + 3 * (order - 2); }
 int force_words(int order) { return 3 * (order / 2); }
@@ -40,12 +41,15 @@ int predmx_ncomp(int order) { return 10 + 3 * (order / 2 - 2); }
 struct hb_ctx {
     int order = 0, nbody = 0, npad = 0;
     int precision = HB_FP64;        // used by the next predict_all
-    int pred_precision = -1;        // layout of the current predicted array
+    int pred_precision = -1;        // precision of the last predict_all
+    double tsys = 0.0;              // time of the last predict_all
+    bool pred_stale = true;         // the predicted array is not at tsys yet
     int R = 0, F = 0;
     int device = 0, nsm = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
 
     double *h_jp = nullptr, *h_force = nullptr, *h_pot = nullptr;
+    double *h_force_dev = nullptr;  // device address of the mapped h_force
     double *d_jp = nullptr, *d_force = nullptr, *d_pot = nullptr, *d_posm = nullptr;
     double *d_partial = nullptr;
     void *d_pred = nullptr;
@@ -60,6 +64,15 @@ struct hb_ctx {
     int njpsend = 0;                // the reference's bookkeeping (previous nact)
     long long launches = 0;
     int variant_override = -1, jsplit_override = 0;
+
+    // device-resident integration (hb_integrator_*)
+    Sched *h_sched = nullptr, *d_sched = nullptr;   // mapped pinned
+    double *d_dt = nullptr;
+    int *d_ilist = nullptr;
+    double *d_epart = nullptr, *h_eout = nullptr, *d_eout = nullptr;
+    cudaGraph_t int_graph = nullptr;
+    cudaGraphExec_t int_exec = nullptr;
+    bool int_ready = false;
     int blocks_per_sm[2][kNumVariants] = {};
     bool smem_set[2][kNumVariants] = {};
     std::string err;
@@ -139,23 +152,71 @@ int sync_stream(hb_ctx *ctx)
     return check_device_flag(ctx);
 }
 
-// Launch shape for the force kernel: variant by nact, then the number of
-// j-slices so that the grid fills the device, each CTA keeps at least a few
-// chunks per warp, and the partials fit in the scratch buffer.
-int pick_variant(const hb_ctx *c, int nact)
+// Launch shapes measured by hermite_b200/autotune.py on a B200, keyed by
+// (order, precision, log2 N bucket, log2 nact bucket).
+struct TuneEntry {
+    int order, mixed, log2n, log2nact, variant, jsplit;
+};
+const TuneEntry kTune[] = {
+#if __has_include("hb_tuning.inc")
+#include "hb_tuning.inc"
+#endif
+    {0, 0, 0, 0, 0, 0}   // end
+};
+
+// Nearest measured bucket: first the nearest N, then the nearest nact.
+const TuneEntry *lookup_tuning(int order, bool mixed, int n, int nact)
 {
+    const double ln = std::log2((double)n), la = std::log2((double)std::max(nact, 1));
+    const TuneEntry *best = nullptr;
+    double bn = 1e30, ba = 1e30;
+    for (const TuneEntry &e : kTune) {
+        if (e.order != order || e.mixed != (mixed ? 1 : 0)) continue;
+        const double dn = std::fabs(e.log2n - ln), da = std::fabs(e.log2nact - la);
+        if (dn < bn - 1e-9 || (dn < bn + 1e-9 && da < ba)) {
+            best = &e;
+            bn = dn;
+            ba = da;
+        }
+    }
+    return best;
+}
+
+// Launch shape for the force kernel: the tuned variant and j-slice count of
+// the nearest bucket (the slice count rescaled to keep the measured number
+// of CTAs), else a heuristic; then the slice count is clamped so that each
+// CTA keeps at least 8 chunks and the partials fit in the scratch buffer.
+int pick_variant(const hb_ctx *c, int nact, int *jsplit_hint)
+{
+    *jsplit_hint = 0;
     if (c->variant_override >= 0) return c->variant_override;
+    const bool mixed = c->pred_precision == HB_MIXED;
+    if (const TuneEntry *e = lookup_tuning(c->order, mixed, c->nbody, nact)) {
+        const ForceVariant *fv = force_variant(c->order, mixed, e->variant);
+        if (fv) {
+            const long long gx_bucket = ((1LL << e->log2nact) + fv->ti - 1) / fv->ti;
+            const long long gx = (nact + fv->ti - 1) / fv->ti;
+            const long long ctas = gx_bucket * e->jsplit;
+            *jsplit_hint = (int)std::max<long long>(1, (ctas + gx - 1) / gx);
+            return e->variant;
+        }
+    }
     if (nact <= 32) return 2;
     if (nact <= 64) return 3;
     if (nact <= c->nsm * 256) return 0;
     return 1;
 }
 
-int run_force(hb_ctx *ctx, int nact, double eps2)
+// Force records up to this size are written by the kernel straight into the
+// mapped pinned buffer (no device->host copy in the block step).
+constexpr size_t kZeroCopyBytes = 256 << 10;
+
+int run_force(hb_ctx *ctx, int nact, double eps2, double *force_out_dev)
 {
     if (nact == 0) return HB_OK;
     const bool mixed = ctx->pred_precision == HB_MIXED;
-    const int v = pick_variant(ctx, nact);
+    int jsplit_hint = 0;
+    const int v = pick_variant(ctx, nact, &jsplit_hint);
     const ForceVariant *fv = force_variant(ctx->order, mixed, v);
     if (!fv) return fail(ctx, HB_ERR_INVALID, "force variant %d does not exist", v);
     const int m = mixed ? 1 : 0;
@@ -169,25 +230,35 @@ int run_force(hb_ctx *ctx, int nact, double eps2)
     }
     const int nchunk = ctx->npad / 32;
     const int gx = (nact + fv->ti - 1) / fv->ti;
-    int S = ctx->jsplit_override;
+    int S = ctx->jsplit_override > 0 ? ctx->jsplit_override : jsplit_hint;
     if (S <= 0) {
         const int target = ctx->nsm * ctx->blocks_per_sm[m][v];
         S = gx >= target ? 1 : (target + gx - 1) / gx;
         // at least 8 chunks (256 j) per CTA and 2 chunks per j-warp
         S = std::min(S, std::max(1, nchunk / std::max(8, 2 * fv->wj)));
     }
-    S = std::max(1, std::min(S, nchunk));
+    S = std::max(1, std::min(S, ctx->jsplit_override > 0 ? nchunk : std::max(1, nchunk / 8)));
     if (S > 1) {
         const size_t need_per_slice = (size_t)gx * fv->ti * ctx->F;
         const size_t smax = ctx->partial_cap / need_per_slice;
         if ((size_t)S > smax) S = (int)std::max<size_t>(1, smax);
     }
+    if (!fv->fused && ctx->pred_stale) {
+        // two-pass shape: the predictor kernel first
+        HB_CK(launch_predict(ctx->order, mixed, ctx->d_jp, ctx->nbody, ctx->npad, ctx->tsys,
+                             ctx->d_pred, ctx->d_err, ctx->stream));
+        ctx->launches++;
+        ctx->pred_stale = false;
+    }
     ForceArgs a;
     a.pred = ctx->d_pred;
+    a.jp = ctx->d_jp;
+    a.tsys = ctx->tsys;
+    a.nbody = ctx->nbody;
     a.nchunk = nchunk;
     a.nact = nact;
     a.eps2 = eps2;
-    a.force = ctx->d_force;
+    a.force = force_out_dev;
     a.partial = ctx->d_partial;
     a.counter = ctx->d_counter;
     a.err = ctx->d_err;
@@ -241,6 +312,13 @@ int hb_destroy(hb_ctx *ctx)
     cudaFree(ctx->d_partial);
     cudaFree(ctx->d_pred);
     cudaFree(ctx->d_counter);
+    if (ctx->int_exec) cudaGraphExecDestroy(ctx->int_exec);
+    if (ctx->int_graph) cudaGraphDestroy(ctx->int_graph);
+    cudaFreeHost(ctx->h_sched);
+    cudaFreeHost(ctx->h_eout);
+    cudaFree(ctx->d_dt);
+    cudaFree(ctx->d_ilist);
+    cudaFree(ctx->d_epart);
     if (ctx->ev_upload) cudaEventDestroy(ctx->ev_upload);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -280,7 +358,8 @@ int hb_create(int order, int nbody, int precision, hb_ctx **out)
     ok = ok && cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&ctx->ev_upload, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaHostAlloc((void **)&ctx->h_jp, np * ctx->R * sizeof(double), cudaHostAllocPortable) == cudaSuccess;
-    ok = ok && cudaHostAlloc((void **)&ctx->h_force, np * ctx->F * sizeof(double), cudaHostAllocPortable) == cudaSuccess;
+    ok = ok && cudaHostAlloc((void **)&ctx->h_force, np * ctx->F * sizeof(double),
+                             cudaHostAllocMapped | cudaHostAllocPortable) == cudaSuccess;
     ok = ok && cudaHostAlloc((void **)&ctx->h_pot, np * sizeof(double), cudaHostAllocPortable) == cudaSuccess;
     ok = ok && cudaHostAlloc((void **)&ctx->h_err, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable) == cudaSuccess;
     ok = ok && cudaMalloc((void **)&ctx->d_jp, np * ctx->R * sizeof(double)) == cudaSuccess;
@@ -291,7 +370,8 @@ int hb_create(int order, int nbody, int precision, hb_ctx **out)
     ok = ok && cudaMalloc(&ctx->d_pred, pred_bytes) == cudaSuccess;
     ok = ok && cudaMalloc((void **)&ctx->d_counter, (np / 32 + 1) * sizeof(unsigned)) == cudaSuccess;
     if (ok) {
-        ok = cudaHostGetDevicePointer((void **)&ctx->d_err, ctx->h_err, 0) == cudaSuccess;
+        ok = cudaHostGetDevicePointer((void **)&ctx->d_err, ctx->h_err, 0) == cudaSuccess &&
+             cudaHostGetDevicePointer((void **)&ctx->h_force_dev, ctx->h_force, 0) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();   // clear the sticky-free error state of the failed call
@@ -352,11 +432,11 @@ int hb_upload(hb_ctx *ctx)
 int hb_predict_all_device(hb_ctx *ctx, double tsys)
 {
     if (!ctx) return HB_ERR_INVALID;
-    const bool mixed = ctx->precision == HB_MIXED;
-    HB_CK(launch_predict(ctx->order, mixed, ctx->d_jp, ctx->nbody, ctx->npad, tsys, ctx->d_pred,
-                         ctx->d_err, ctx->stream));
-    ctx->launches++;
+    // The prediction itself runs with the next force launch: inside the fused
+    // force kernel, or as a predictor pass ahead of a two-pass force kernel.
+    ctx->tsys = tsys;
     ctx->pred_precision = ctx->precision;
+    ctx->pred_stale = true;
     return HB_OK;
 }
 
@@ -376,7 +456,7 @@ int hb_force_device(hb_ctx *ctx, int nact, double eps2)
     if (!(eps2 >= 0.0)) return fail(ctx, HB_ERR_INVALID, "eps2 must be >= 0");
     if (ctx->pred_precision < 0)
         return fail(ctx, HB_ERR_STATE, "calc_force_on_first_nact before any predict_all");
-    return run_force(ctx, nact, eps2);
+    return run_force(ctx, nact, eps2, ctx->d_force);
 }
 
 int hb_download_forces(hb_ctx *ctx, int nact, double *force_out)
@@ -396,10 +476,24 @@ int hb_force_first_nact(hb_ctx *ctx, int nact, double eps2, double *force_out)
 {
     if (!ctx) return HB_ERR_INVALID;
     if (nact > 0 && !force_out) return fail(ctx, HB_ERR_INVALID, "force_out is NULL");
-    int s = hb_force_device(ctx, nact, eps2);
-    if (s != HB_OK) return s;
-    s = hb_download_forces(ctx, nact, force_out);
-    if (s != HB_OK) return s;
+    int s;
+    if ((size_t)nact * ctx->F * sizeof(double) <= kZeroCopyBytes) {
+        // small block step: the kernel writes the records into pinned host
+        // memory itself; only the stream synchronisation remains
+        if (nact < 0 || nact > ctx->nbody)
+            return fail(ctx, HB_ERR_INVALID, "nact=%d outside [0, %d]", nact, ctx->nbody);
+        if (!(eps2 >= 0.0)) return fail(ctx, HB_ERR_INVALID, "eps2 must be >= 0");
+        if (ctx->pred_precision < 0)
+            return fail(ctx, HB_ERR_STATE, "calc_force_on_first_nact before any predict_all");
+        s = run_force(ctx, nact, eps2, ctx->h_force_dev);
+        if (s == HB_OK) s = sync_stream(ctx);
+        if (s != HB_OK) return s;
+        if (nact > 0) std::memcpy(force_out, ctx->h_force, sizeof(double) * (size_t)nact * ctx->F);
+    } else {
+        s = hb_force_device(ctx, nact, eps2);
+        if (s == HB_OK) s = hb_download_forces(ctx, nact, force_out);
+        if (s != HB_OK) return s;
+    }
     ctx->njpsend = nact;
     return HB_OK;
 }
@@ -477,6 +571,192 @@ int hb_force_variant_info(int order, int precision, int variant, int *threads, i
     if (threads) *threads = fv->nw * 32;
     if (i_per_thread) *i_per_thread = fv->ni;
     if (j_warps) *j_warps = fv->wj;
+    return HB_OK;
+}
+
+// ---- device-resident integration -------------------------------------------
+namespace {
+constexpr int kStepsPerGraph = 32;
+constexpr int kEnergyParts = 256;
+
+int integrator_alloc(hb_ctx *ctx)
+{
+    if (ctx->h_sched) return HB_OK;
+    const size_t np = ctx->npad;
+    bool ok = cudaHostAlloc((void **)&ctx->h_sched, sizeof(Sched), cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer((void **)&ctx->d_sched, ctx->h_sched, 0) == cudaSuccess &&
+              cudaHostAlloc((void **)&ctx->h_eout, 2 * sizeof(double), cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer((void **)&ctx->d_eout, ctx->h_eout, 0) == cudaSuccess &&
+              cudaMalloc((void **)&ctx->d_dt, np * sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void **)&ctx->d_ilist, np * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&ctx->d_epart, 2 * kEnergyParts * sizeof(double)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        return fail(ctx, HB_ERR_ALLOC, "integrator buffers could not be allocated");
+    }
+    return HB_OK;
+}
+}  // namespace
+
+int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double eta_s, double dtmax)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    if (!(eps2 >= 0.0) || !(eta > 0.0) || !(eta_s > 0.0) || !(dtmax > 0.0) ||
+        std::log2(dtmax) != std::floor(std::log2(dtmax)) || !(tsys >= 0.0))
+        return fail(ctx, HB_ERR_INVALID, "integrator_init: need eps2 >= 0, eta, eta_s > 0, "
+                                         "dtmax a power of two, tsys >= 0");
+    int s = integrator_alloc(ctx);
+    if (s != HB_OK) return s;
+    s = sync_stream(ctx);
+    if (s != HB_OK) return s;
+    if (ctx->int_exec) { cudaGraphExecDestroy(ctx->int_exec); ctx->int_exec = nullptr; }
+    if (ctx->int_graph) { cudaGraphDestroy(ctx->int_graph); ctx->int_graph = nullptr; }
+    ctx->int_ready = false;
+
+    // initial conditions: the mirror's pos, mass, vel at tlast = tsys, all
+    // derivatives zero (the reference's Particle constructor), as in
+    // NbodySystem::init_step (SRC/nbodysystem.h:565-631)
+    for (int i = 0; i < ctx->nbody; ++i) {
+        double *r = ctx->h_jp + (size_t)i * ctx->R;
+        r[7] = tsys;
+        std::memset(r + 8, 0, sizeof(double) * (ctx->R - 8));
+    }
+    mark_dirty(ctx, 0, ctx->nbody);
+    s = do_upload(ctx);
+    if (s != HB_OK) return s;
+    const int passes = ctx->order > 4 ? 2 : 1;   // higher derivatives bootstrap
+    for (int p = 0; p < passes; ++p) {
+        hb_predict_all_device(ctx, tsys);
+        s = run_force(ctx, ctx->nbody, eps2, ctx->d_force);
+        if (s != HB_OK) return s;
+        HB_CK(integrator_assign(ctx->order, ctx->d_jp, ctx->d_dt, ctx->d_force, ctx->nbody,
+                                p == passes - 1, eta_s, dtmax, ctx->stream));
+        ctx->launches++;
+    }
+    s = sync_stream(ctx);
+    if (s != HB_OK) return s;
+
+    Sched &sc = *ctx->h_sched;
+    std::memset(&sc, 0, sizeof(Sched));
+    sc.tnext_bits = 0x7ff0000000000000ull;
+    sc.tsys = tsys;
+    sc.tend = tsys;
+    sc.eps2 = eps2;
+    sc.etapow = std::pow(eta, 2.0 * (ctx->order - 3));   // set_run_params, SRC/nbodysystem.h:472
+    sc.dtmax = dtmax;
+
+    IntegratorLaunch L;
+    L.jp = ctx->d_jp;
+    L.dt = ctx->d_dt;
+    L.ilist = ctx->d_ilist;
+    L.sched = ctx->d_sched;
+    L.force = ctx->d_force;
+    L.partial = ctx->d_partial;
+    L.counter = ctx->d_counter;
+    L.err = ctx->d_err;
+    L.n = ctx->nbody;
+    L.nchunk = ctx->npad / 32;
+    L.nsm = ctx->nsm;
+    L.partial_cap = ctx->partial_cap;
+    L.mixed = ctx->precision == HB_MIXED;
+    int smem = 0, per_sm = 0;
+    HB_CK(integrator_kernel_setup(ctx->order, L.mixed, &smem, &per_sm));
+    L.smem_fp64 = L.smem_mixed = smem;
+    L.items_grid = ctx->nsm * std::max(1, per_sm);
+    L.target_items = 2 * L.items_grid;
+
+    if (ctx->stream == nullptr) return fail(ctx, HB_ERR_STATE, "integrator needs a non-default stream");
+    HB_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = cudaSuccess;
+    for (int k = 0; k < kStepsPerGraph && ce == cudaSuccess; ++k)
+        ce = integrator_step_launch(ctx->order, L, ctx->stream);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &graph);
+    if (ce != cudaSuccess || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(ctx, HB_ERR_CUDA, "capturing the block-step graph failed: %s",
+                    cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+    }
+    ctx->int_graph = graph;
+    HB_CK(cudaGraphInstantiate(&ctx->int_exec, graph, 0));
+    ctx->int_ready = true;
+    ctx->pred_precision = ctx->precision;
+    return HB_OK;
+}
+
+int hb_integrator_run(hb_ctx *ctx, double tend, long long max_block_steps)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    if (!ctx->int_ready) return fail(ctx, HB_ERR_STATE, "hb_integrator_run before hb_integrator_init");
+    int s = sync_stream(ctx);
+    if (s != HB_OK) return s;
+    volatile Sched *sc = ctx->h_sched;
+    if (!(tend >= sc->tsys)) return fail(ctx, HB_ERR_INVALID, "tend %g is before tsys %g", tend, sc->tsys);
+    sc->tend = tend;
+    long long last_steps = sc->block_steps;
+    const long long first_steps = sc->block_steps;
+    for (long long launch = 0; sc->tsys < tend; ++launch) {
+        if (max_block_steps > 0 && sc->block_steps - first_steps >= max_block_steps)
+            return fail(ctx, HB_ERR_STATE, "block-step limit %lld reached at t = %.17g",
+                        max_block_steps, sc->tsys);
+        HB_CK(cudaGraphLaunch(ctx->int_exec, ctx->stream));
+        ctx->launches += 4LL * kStepsPerGraph;
+        s = sync_stream(ctx);
+        if (s != HB_OK) return s;
+        if (sc->error)
+            return fail(ctx, sc->error == 2 ? HB_ERR_DEVICE_TIMEOUT : HB_ERR_STATE,
+                        sc->error == 2 ? "a device-side wait gave up" : "a timestep underflowed (< 2^-48)");
+        if (sc->block_steps == last_steps && sc->tsys < tend)
+            return fail(ctx, HB_ERR_STATE, "integration stalled at t = %.17g", sc->tsys);
+        last_steps = sc->block_steps;
+    }
+    return HB_OK;
+}
+
+int hb_integrator_stats(const hb_ctx *ctx, long long *particle_steps, long long *block_steps,
+                        double *tsys)
+{
+    if (!ctx || !ctx->h_sched) return HB_ERR_INVALID;
+    const volatile Sched *sc = ctx->h_sched;
+    if (particle_steps) *particle_steps = sc->particle_steps;
+    if (block_steps) *block_steps = sc->block_steps;
+    if (tsys) *tsys = sc->tsys;
+    return HB_OK;
+}
+
+int hb_energy(hb_ctx *ctx, double eps2, double *kinetic, double *potential)
+{
+    if (!ctx || !kinetic || !potential) return HB_ERR_INVALID;
+    if (!(eps2 >= 0.0)) return fail(ctx, HB_ERR_INVALID, "eps2 must be >= 0");
+    int s = integrator_alloc(ctx);
+    if (s == HB_OK) s = do_upload(ctx);
+    if (s != HB_OK) return s;
+    HB_CK(launch_potential(ctx->order, ctx->d_jp, ctx->nbody, ctx->npad, eps2, ctx->d_posm,
+                           ctx->d_pot, ctx->d_err, ctx->stream));
+    HB_CK(integrator_energy(ctx->order, ctx->d_jp, ctx->d_pot, ctx->nbody, ctx->d_epart,
+                            ctx->d_eout, ctx->stream));
+    ctx->launches += 4;
+    s = sync_stream(ctx);
+    if (s != HB_OK) return s;
+    *kinetic = ctx->h_eout[0];
+    *potential = ctx->h_eout[1];
+    return HB_OK;
+}
+
+int hb_get_records(hb_ctx *ctx, int addr0, int count, double *records_out, double *dt_out)
+{
+    if (!ctx || addr0 < 0 || count < 0 || (long long)addr0 + count > ctx->nbody ||
+        (count > 0 && !records_out))
+        return HB_ERR_INVALID;
+    int s = sync_stream(ctx);
+    if (s != HB_OK || count == 0) return s;
+    HB_CK(cudaMemcpy(records_out, ctx->d_jp + (size_t)addr0 * ctx->R,
+                     sizeof(double) * (size_t)count * ctx->R, cudaMemcpyDeviceToHost));
+    if (dt_out) {
+        if (!ctx->d_dt) return fail(ctx, HB_ERR_STATE, "no timesteps before hb_integrator_init");
+        HB_CK(cudaMemcpy(dt_out, ctx->d_dt + addr0, sizeof(double) * (size_t)count,
+                         cudaMemcpyDeviceToHost));
+    }
     return HB_OK;
 }
 

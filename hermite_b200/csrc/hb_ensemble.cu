@@ -1,0 +1,823 @@
+// hb_ensemble.cu -- batched ensembles of independent clusters on one GPU.
+//
+// Many small N-body systems (different N, masses, softenings) advanced
+// together: one global block-step loop over the union of their particles,
+// each particle interacting only with its own cluster.  Clusters are laid
+// end to end in one record array, each padded to a multiple of 128 slots
+// with inert padding (zero mass, far-away positions, dt = +inf, so never
+// active and contributing exactly zero).  Per block step, all on the device
+// and replayed from a captured CUDA graph:
+//   1. tnext = min over all slots of (tlast + dt); per-cluster counters reset
+//   2. active slots compacted into their cluster's own slot range
+//      (ilist[off_c + k]), then one CTA turns the per-cluster counts into
+//      i-tile offsets
+//   3. one work-item force launch over every cluster's i-tiles x j-slices,
+//      each tile against its own cluster's j range and softening
+//   4. the Hermite corrector (shared with the single-system integrator)
+// This is the batching form of the reference's integrator: no reference
+// counterpart exists (the reference runs one system per process).
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hermite_b200.h"
+#include "hb_common.cuh"
+#include "hb_corrector.cuh"
+#include "hb_force.cuh"
+#include "hb_internal.h"
+
+namespace hb {
+namespace {
+
+constexpr int kClusterPad = 128;
+constexpr int kMaxClusters = 4096;
+constexpr unsigned long long kInf = 0x7ff0000000000000ull;
+
+struct Cluster {
+    int off, n, npad, pad;
+    double eps2;
+};
+
+struct EnsSched {
+    unsigned long long tnext_bits;
+    int work, error, total_tiles, nact;
+    double tnext, dtlim, tsys, tend;
+    double etapow, dtmax;
+    long long particle_steps, block_steps;
+    double interactions;
+};
+
+struct EnsLaunch {
+    double *jp, *dt, *force, *partial;
+    int *ilist, *ccnt, *tile_base;     // tile_base[nclusters + 1]
+    unsigned *counter;
+    const Cluster *cl;
+    const int *slot_cluster;           // per 128-slot block
+    EnsSched *s;
+    int *err;
+    int nslot, nclusters, nsm;
+    size_t partial_cap;
+    int target_items, items_grid, smem;
+};
+
+// 1. next block time; reset the per-cluster counters
+template <int ORDER>
+__global__ void ens_min_kernel(EnsLaunch L)
+{
+    constexpr int R = Rec<ORDER>::words;
+    double m = __longlong_as_double((long long)kInf);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.nslot; i += gridDim.x * blockDim.x)
+        m = fmin(m, L.dt[i] + L.jp[(size_t)i * R + 7]);
+    for (int o = 16; o; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double wm[32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? wm[threadIdx.x] : __longlong_as_double((long long)kInf);
+        for (int o = 16; o; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) atomicMin(&L.s->tnext_bits, (unsigned long long)__double_as_longlong(m));
+    }
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < L.nclusters; c += gridDim.x * blockDim.x)
+        L.ccnt[c] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) L.s->work = 0;
+}
+
+// 2a. active slots into their cluster's range
+template <int ORDER>
+__global__ void ens_compact_kernel(EnsLaunch L)
+{
+    constexpr int R = Rec<ORDER>::words;
+    const double tnext = __longlong_as_double((long long)L.s->tnext_bits);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double dtlim = L.s->dtmax, q = tnext / L.s->dtmax;
+        for (int k = 0; k < 64 && q != trunc(q); ++k) {
+            q *= 2.0;
+            dtlim *= 0.5;
+        }
+        L.s->tnext = tnext;
+        L.s->dtlim = dtlim;
+    }
+    if (!(tnext <= L.s->tend) || L.s->error) return;
+    for (int base = blockIdx.x * blockDim.x; base < L.nslot; base += gridDim.x * blockDim.x) {
+        const int i = base + threadIdx.x;   // blockDim 128: one cluster per block
+        const int c = L.slot_cluster[base / kClusterPad];
+        const bool act = i < L.nslot && L.dt[i] + L.jp[(size_t)i * R + 7] == tnext;
+        const unsigned ballot = __ballot_sync(0xffffffffu, act);
+        int off = 0;
+        if ((threadIdx.x & 31) == 0 && ballot) off = atomicAdd(&L.ccnt[c], __popc(ballot));
+        off = __shfl_sync(0xffffffffu, off, 0);
+        if (act) L.ilist[L.cl[c].off + off + __popc(ballot & ((1u << (threadIdx.x & 31)) - 1u))] = i;
+    }
+}
+
+// 2b. per-cluster i-tile offsets (one CTA)
+__global__ void ens_tiles_kernel(EnsLaunch L)
+{
+    __shared__ int part[1024];
+    const int per = (L.nclusters + blockDim.x - 1) / blockDim.x;
+    const int c0 = threadIdx.x * per, c1 = min(L.nclusters, c0 + per);
+    int tiles = 0, act = 0;
+    for (int c = c0; c < c1; ++c) {
+        tiles += (L.ccnt[c] + 31) / 32;
+        act += L.ccnt[c];
+    }
+    part[threadIdx.x] = tiles;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int t = 0; t < (int)blockDim.x; ++t) {
+            const int v = part[t];
+            part[t] = run;
+            run += v;
+        }
+        L.s->total_tiles = run;
+    }
+    __syncthreads();
+    int run = part[threadIdx.x];
+    for (int c = c0; c < c1; ++c) {
+        L.tile_base[c] = run;
+        run += (L.ccnt[c] + 31) / 32;
+    }
+    if (threadIdx.x == blockDim.x - 1) L.tile_base[L.nclusters] = run;
+    // totals for the statistics
+    __shared__ int sact[1024];
+    sact[threadIdx.x] = act;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long tot = 0;
+        double inter = 0.0;
+        for (int t = 0; t < (int)blockDim.x; ++t) tot += sact[t];
+        for (int c = 0; c < L.nclusters; ++c) inter += (double)L.ccnt[c] * L.cl[c].n;
+        L.s->nact = (int)tot;
+        if (tot > 0) {
+            L.s->particle_steps += tot;
+            L.s->block_steps += 1;
+            L.s->interactions += inter;
+        }
+    }
+}
+
+// 3. fused predict + force over (tile, j-slice) items of all clusters
+template <int ORDER, bool MIXED>
+__global__ void __launch_bounds__(128)
+ens_force_kernel(EnsLaunch L)
+{
+    constexpr int NW = 4, WJ = 4, TCH = 4, STG = 2, TI = 32;
+    constexpr int F = Frc<ORDER>::words, R = Rec<ORDER>::words, RB = Rec<ORDER>::bytes;
+    using Sh = ForceShape<ORDER, MIXED, NW, 1, WJ, TCH, true>;
+    constexpr int CB = Sh::CB;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::body_bytes);
+    unsigned char *ptile = smem + Sh::ring_bytes;
+    __shared__ int s_item;
+    __shared__ unsigned s_last;
+
+    const int T = L.s->total_tiles;
+    if (T == 0) return;
+    const double tsys = L.s->tnext;
+    const int tid = threadIdx.x, lane = tid & 31, jg = tid >> 5;
+    int S = (L.target_items + T - 1) / T;
+    S = max(1, min(S, 16));
+    while (S > 1 && (size_t)S * T * TI * F > L.partial_cap) --S;
+    const int items = T * S;
+    const size_t tspan = (size_t)T * TI;
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned g = 0;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(&L.s->work, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= items) break;
+        const int tile = item / S, sl = item % S;
+        // the tile's cluster: last c with tile_base[c] <= tile
+        int lo = 0, hi = L.nclusters - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (L.tile_base[mid] <= tile) lo = mid; else hi = mid - 1;
+        }
+        const int c = lo;
+        const Cluster cl = L.cl[c];
+        const int cnt = L.ccnt[c];
+        const int k0 = (tile - L.tile_base[c]) * TI;
+        const double eps2 = cl.eps2;
+
+        double *raw = reinterpret_cast<double *>(smem);
+        for (int w = tid; w < TI * R; w += NW * 32) {
+            const int q = w / R, k = k0 + q;
+            const int slot = L.ilist[cl.off + (k < cnt ? k : cnt - 1)];
+            raw[w] = L.jp[(size_t)slot * R + (w - q * R)];
+        }
+        __syncthreads();
+        predict_tile<ORDER, MIXED>(raw, TI, 0, INT_MAX, tsys, ptile);
+        __syncthreads();
+        using IBody = typename std::conditional<MIXED, NegI32, Body64>::type;
+        IBody I[1];
+        if constexpr (MIXED) load_i_mixed<ORDER>(reinterpret_cast<const float *>(ptile), 0, lane, I[0]);
+        else load_i64<ORDER>(reinterpret_cast<const double *>(ptile), 0, lane, I[0]);
+        __syncthreads();
+
+        double f[1][F];
+#pragma unroll
+        for (int q = 0; q < F; ++q) f[0][q] = 0.0;
+        const int cb = cl.off / 32, nch = cl.npad / 32;
+        const int c0 = cb + (int)(((long long)sl * nch) / S);
+        const int c1 = cb + (int)(((long long)(sl + 1) * nch) / S);
+        const int ntile = (c1 - c0 + TCH - 1) / TCH;
+        auto issue = [&](int t) {
+            const unsigned gt = g + t;
+            const int st = gt % STG;
+            const int cs = c0 + t * TCH, cc = min(TCH, c1 - cs);
+            const uint32_t bytes = (uint32_t)(cc * 32 * RB);
+            mbar_arrive_expect_tx(&bar[st], bytes);
+            bulk_load(smem + st * Sh::tile_bytes, L.jp + (size_t)cs * 32 * R, bytes, &bar[st]);
+        };
+        if (tid == 0)
+            for (int t = 0; t < STG && t < ntile; ++t) issue(t);
+        const float2 eps2f = f2((float)eps2);
+        int failed_at = -1;
+        for (int t = 0; t < ntile; ++t) {
+            const unsigned gt = g + t;
+            const int st = gt % STG;
+            const bool got = mbar_wait_bounded(&bar[st], (gt / STG) & 1u);
+            if (!__syncthreads_and(got)) { failed_at = t; break; }
+            const int cc = min(TCH, c1 - (c0 + t * TCH));
+            // padding records are inert (zero mass, far away): no slot test
+            predict_tile<ORDER, MIXED>(reinterpret_cast<const double *>(smem + st * Sh::tile_bytes),
+                                       cc * 32, 0, INT_MAX, tsys, ptile);
+            __syncthreads();
+            if (tid == 0 && t + STG < ntile) issue(t + STG);
+            for (int q = jg; q < cc; q += WJ) {
+                if constexpr (MIXED)
+                    chunk_mixed<ORDER, 1, (HB_MIXED_REFINE != 0)>(reinterpret_cast<const float *>(ptile + q * CB), I, eps2f, f);
+                else
+                    chunk64<ORDER, 1>(reinterpret_cast<const double *>(ptile + q * CB), I, eps2, f);
+            }
+            __syncthreads();
+        }
+        if (failed_at >= 0) {
+            if (tid == 0) {
+                raise_error(L.err, kErrWaitTimeout);
+                for (int t = failed_at; t < ntile && t < failed_at + STG; ++t)
+                    mbar_wait_bounded(&bar[(g + t) % STG], ((g + t) / STG) & 1u);
+            }
+            L.s->error = 2;
+            return;
+        }
+        g += ntile;
+
+        double *red = reinterpret_cast<double *>(smem);
+        if (jg > 0)
+#pragma unroll
+            for (int q = 0; q < F; ++q) red[((jg - 1) * F + q) * 32 + lane] = f[0][q];
+        __syncthreads();
+        const int k = k0 + lane;
+        const size_t pos = (size_t)cl.off + k;   // force row = ilist position
+        if (jg == 0) {
+            for (int w = 1; w < WJ; ++w)
+#pragma unroll
+                for (int q = 0; q < F; ++q) f[0][q] += red[((w - 1) * F + q) * 32 + lane];
+            if (S == 1) {
+                if (k < cnt)
+#pragma unroll
+                    for (int q = 0; q < F; ++q) L.force[pos * F + q] = f[0][q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < F; ++q)
+                    L.partial[((size_t)sl * tspan + (size_t)tile * TI + lane) * F + q] = f[0][q];
+            }
+        }
+        if (S > 1) {
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) s_last = (atomicAdd(&L.counter[tile], 1u) == (unsigned)(S - 1));
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                const int V = min(TI, cnt - k0) * F;
+                const double *pbase = L.partial + (size_t)tile * TI * F;
+                for (int e = tid; e < V; e += NW * 32) {
+                    double sum = 0.0;
+                    for (int s2 = 0; s2 < S; ++s2) sum += __ldcg(pbase + (size_t)s2 * tspan * F + e);
+                    L.force[((size_t)cl.off + k0) * F + e] = sum;
+                }
+                if (tid == 0) L.counter[tile] = 0u;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// 4. corrector over every cluster's active list
+template <int ORDER>
+__global__ void ens_correct_kernel(EnsLaunch L)
+{
+    constexpr int R = Rec<ORDER>::words, F = Frc<ORDER>::words;
+    const int T = L.s->total_tiles;
+    const double dtlim = L.s->dtlim, etapow = L.s->etapow;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < T * 32; p += gridDim.x * blockDim.x) {
+        const int tile = p >> 5;
+        int lo = 0, hi = L.nclusters - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (L.tile_base[mid] <= tile) lo = mid; else hi = mid - 1;
+        }
+        const int k = (tile - L.tile_base[lo]) * 32 + (p & 31);
+        if (k >= L.ccnt[lo]) continue;
+        const size_t pos = (size_t)L.cl[lo].off + k;
+        const int i = L.ilist[pos];
+        const double dtn = correct_particle<ORDER>(L.jp + (size_t)i * R, L.force + pos * F, L.dt[i],
+                                                   etapow, dtlim);
+        if (!(dtn >= 0x1p-48)) L.s->error = 1;
+        L.dt[i] = dtn;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (L.s->nact > 0) L.s->tsys = L.s->tnext;
+        L.s->tnext_bits = kInf;
+    }
+}
+
+// initialisation: every real slot active (no dt yet), forces written into the
+// records, dt from init_dt on the last pass
+__global__ void ens_all_active_kernel(EnsLaunch L)
+{
+    for (int c = blockIdx.x; c < L.nclusters; c += gridDim.x) {
+        const Cluster cl = L.cl[c];
+        for (int k = threadIdx.x; k < cl.n; k += blockDim.x) L.ilist[cl.off + k] = cl.off + k;
+        if (threadIdx.x == 0) L.ccnt[c] = cl.n;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) L.s->work = 0;
+}
+
+template <int ORDER>
+__global__ void ens_assign_kernel(EnsLaunch L, int set_dt, double eta_s)
+{
+    constexpr int R = Rec<ORDER>::words, F = Frc<ORDER>::words;
+    for (int c = blockIdx.x; c < L.nclusters; c += gridDim.x) {
+        const Cluster cl = L.cl[c];
+        for (int k = threadIdx.x; k < cl.n; k += blockDim.x) {
+            const size_t i = (size_t)cl.off + k;
+            for (int q = 0; q < F; ++q) L.jp[i * R + 8 + q] = L.force[i * F + q];
+            if (set_dt) L.dt[i] = initial_dt<ORDER>(L.force + i * F, eta_s, L.s->dtmax);
+        }
+    }
+}
+
+// potential per cluster (FP64), then per-cluster kinetic / potential sums
+template <int ORDER>
+__global__ void ens_potential_kernel(EnsLaunch L, double *pot)
+{
+    constexpr int R = Rec<ORDER>::words;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;       // blockDim 128
+    const Cluster cl = L.cl[L.slot_cluster[blockIdx.x * blockDim.x / kClusterPad]];
+    const double *ri = L.jp + (size_t)i * R;
+    double sum = 0.0;
+    for (int j = cl.off; j < cl.off + cl.n; ++j) {
+        const double *rj = L.jp + (size_t)j * R;
+        const double dx = rj[0] - ri[0], dy = rj[1] - ri[1], dz = rj[2] - ri[2];
+        const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, cl.eps2)));
+        if (j != i) sum = fma(-rj[3], rsqrt_fp64(r2), sum);
+    }
+    pot[i] = sum;
+}
+
+template <int ORDER>
+__global__ void ens_energy_kernel(EnsLaunch L, const double *pot, double *out)
+{
+    constexpr int R = Rec<ORDER>::words;
+    const Cluster cl = L.cl[blockIdx.x];
+    double ke = 0.0, pe = 0.0;
+    for (int k = threadIdx.x; k < cl.n; k += blockDim.x) {
+        const double *r = L.jp + (size_t)(cl.off + k) * R;
+        ke += r[3] * (r[4] * r[4] + r[5] * r[5] + r[6] * r[6]);
+        pe += r[3] * pot[cl.off + k];
+    }
+    __shared__ double sk[256], sp[256];
+    sk[threadIdx.x] = ke;
+    sp[threadIdx.x] = pe;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o; o >>= 1) {
+        if (threadIdx.x < o) {
+            sk[threadIdx.x] += sk[threadIdx.x + o];
+            sp[threadIdx.x] += sp[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[2 * blockIdx.x] = 0.5 * sk[0];
+        out[2 * blockIdx.x + 1] = 0.5 * sp[0];
+    }
+}
+
+template <int ORDER>
+cudaError_t ens_step(const EnsLaunch &L, bool mixed, cudaStream_t s)
+{
+    const int nb = std::max(1, std::min((L.nslot + 127) / 128, L.nsm * 8));
+    ens_min_kernel<ORDER><<<nb, 256, 0, s>>>(L);
+    ens_compact_kernel<ORDER><<<nb, 128, 0, s>>>(L);
+    ens_tiles_kernel<<<1, 256, 0, s>>>(L);
+    if (mixed) ens_force_kernel<ORDER, true><<<L.items_grid, 128, L.smem, s>>>(L);
+    else ens_force_kernel<ORDER, false><<<L.items_grid, 128, L.smem, s>>>(L);
+    ens_correct_kernel<ORDER><<<L.nsm * 4, 128, 0, s>>>(L);
+    return cudaGetLastError();
+}
+
+template <int ORDER>
+cudaError_t ens_force_all(const EnsLaunch &L, bool mixed, int set_dt, double eta_s, cudaStream_t s)
+{
+    ens_all_active_kernel<<<std::min(L.nclusters, 1024), 256, 0, s>>>(L);
+    ens_tiles_kernel<<<1, 256, 0, s>>>(L);
+    if (mixed) ens_force_kernel<ORDER, true><<<L.items_grid, 128, L.smem, s>>>(L);
+    else ens_force_kernel<ORDER, false><<<L.items_grid, 128, L.smem, s>>>(L);
+    ens_assign_kernel<ORDER><<<std::min(L.nclusters, 1024), 256, 0, s>>>(L, set_dt, eta_s);
+    return cudaGetLastError();
+}
+
+template <int ORDER>
+cudaError_t ens_energy(const EnsLaunch &L, double *pot, double *out, cudaStream_t s)
+{
+    ens_potential_kernel<ORDER><<<L.nslot / 128, 128, 0, s>>>(L, pot);
+    ens_energy_kernel<ORDER><<<L.nclusters, 256, 0, s>>>(L, pot, out);
+    return cudaGetLastError();
+}
+
+template <int ORDER, bool M>
+cudaError_t ens_setup(int *smem, int *per_sm)
+{
+    const void *k = (const void *)&ens_force_kernel<ORDER, M>;
+    *smem = ForceShape<ORDER, M, 4, 1, 4, 4, true>::smem_bytes;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, 128, *smem);
+}
+
+}  // namespace
+}  // namespace hb
+
+using namespace hb;
+
+struct hb_ens {
+    int order = 0, precision = 0, nclusters = 0, nslot = 0, R = 0, F = 0, nsm = 0;
+    std::vector<Cluster> cl;
+    cudaStream_t stream = nullptr;
+    double *d_jp = nullptr, *d_dt = nullptr, *d_force = nullptr, *d_partial = nullptr,
+           *d_pot = nullptr, *h_eout = nullptr, *d_eout = nullptr;
+    int *d_ilist = nullptr, *d_ccnt = nullptr, *d_tile_base = nullptr, *d_slot_cluster = nullptr;
+    unsigned *d_counter = nullptr;
+    Cluster *d_cl = nullptr;
+    EnsSched *h_s = nullptr, *d_s = nullptr;
+    int *h_err = nullptr, *d_err = nullptr;
+    size_t partial_cap = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ready = false;
+    std::string err;
+    EnsLaunch L;
+};
+
+namespace {
+constexpr int kEnsStepsPerGraph = 32;
+
+int ens_fail(hb_ens *e, int status, const char *msg, cudaError_t ce = cudaSuccess)
+{
+    if (e) {
+        e->err = msg;
+        if (ce != cudaSuccess) {
+            e->err += ": ";
+            e->err += cudaGetErrorString(ce);
+        }
+    }
+    return status;
+}
+
+cudaError_t dispatch_step(hb_ens *e)
+{
+    const bool m = e->precision == HB_MIXED;
+    switch (e->order) {
+    case 4: return ens_step<4>(e->L, m, e->stream);
+    case 6: return ens_step<6>(e->L, m, e->stream);
+    case 8: return ens_step<8>(e->L, m, e->stream);
+    }
+    return cudaErrorInvalidValue;
+}
+}  // namespace
+
+extern "C" {
+
+int hb_ens_destroy(hb_ens *e)
+{
+    if (!e) return HB_OK;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    cudaFree(e->d_jp);
+    cudaFree(e->d_dt);
+    cudaFree(e->d_force);
+    cudaFree(e->d_partial);
+    cudaFree(e->d_pot);
+    cudaFree(e->d_ilist);
+    cudaFree(e->d_ccnt);
+    cudaFree(e->d_tile_base);
+    cudaFree(e->d_slot_cluster);
+    cudaFree(e->d_counter);
+    cudaFree(e->d_cl);
+    cudaFreeHost(e->h_s);
+    cudaFreeHost(e->h_eout);
+    cudaFreeHost(e->h_err);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return HB_OK;
+}
+
+int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_ens **out)
+{
+    if (!out) return HB_ERR_INVALID;
+    *out = nullptr;
+    if ((order != 4 && order != 6 && order != 8) || nclusters < 1 || nclusters > kMaxClusters ||
+        !sizes || (precision != HB_FP64 && precision != HB_MIXED))
+        return HB_ERR_INVALID;
+    long long total = 0;
+    for (int c = 0; c < nclusters; ++c) {
+        if (sizes[c] < 1) return HB_ERR_INVALID;
+        total += (sizes[c] + kClusterPad - 1) / kClusterPad * kClusterPad;
+    }
+    if (total > (1LL << 26)) return HB_ERR_TOO_LARGE;
+    int dev = 0;
+    cudaDeviceProp prop;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess ||
+        prop.major != 10 || prop.minor != 0)
+        return HB_ERR_NO_DEVICE;
+
+    hb_ens *e = new hb_ens;
+    e->order = order;
+    e->precision = precision;
+    e->nclusters = nclusters;
+    e->nslot = (int)total;
+    e->R = 8 + 3 * (order - 2);
+    e->F = 3 * (order / 2);
+    e->nsm = prop.multiProcessorCount;
+    int off = 0;
+    std::vector<int> slot_cluster(total / kClusterPad);
+    for (int c = 0; c < nclusters; ++c) {
+        Cluster k;
+        k.off = off;
+        k.n = sizes[c];
+        k.npad = (sizes[c] + kClusterPad - 1) / kClusterPad * kClusterPad;
+        k.pad = 0;
+        k.eps2 = 0.0;
+        for (int b = off / kClusterPad; b < (off + k.npad) / kClusterPad; ++b) slot_cluster[b] = c;
+        e->cl.push_back(k);
+        off += k.npad;
+    }
+    const size_t ns = e->nslot;
+    e->partial_cap = (size_t)2 * e->nsm * 8 * 256 * e->F;
+    bool ok = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_jp, ns * e->R * sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_dt, ns * sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_force, ns * e->F * sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_partial, e->partial_cap * sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_pot, ns * sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_ilist, ns * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_ccnt, nclusters * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_tile_base, (nclusters + 1) * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_slot_cluster, slot_cluster.size() * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_counter, (ns / 32 + nclusters + 1) * sizeof(unsigned)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_cl, nclusters * sizeof(Cluster)) == cudaSuccess &&
+              cudaHostAlloc((void **)&e->h_s, sizeof(EnsSched), cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer((void **)&e->d_s, e->h_s, 0) == cudaSuccess &&
+              cudaHostAlloc((void **)&e->h_eout, 2 * nclusters * sizeof(double), cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer((void **)&e->d_eout, e->h_eout, 0) == cudaSuccess &&
+              cudaHostAlloc((void **)&e->h_err, sizeof(int), cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer((void **)&e->d_err, e->h_err, 0) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        hb_ens_destroy(e);
+        return HB_ERR_ALLOC;
+    }
+    *e->h_err = 0;
+    std::memset(e->h_s, 0, sizeof(EnsSched));
+    e->h_s->tnext_bits = kInf;
+    // inert padding everywhere until clusters are set
+    std::vector<double> pad(ns * e->R, 0.0);
+    std::vector<double> dt(ns, INFINITY);
+    for (size_t i = 0; i < ns; ++i)
+        for (int k = 0; k < 3; ++k) pad[i * e->R + k] = 1099511627776.0 + (double)(i * 3 + k);
+    ok = cudaMemcpy(e->d_jp, pad.data(), pad.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(e->d_dt, dt.data(), dt.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(e->d_slot_cluster, slot_cluster.data(), slot_cluster.size() * sizeof(int),
+                    cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(e->d_counter, 0, (ns / 32 + nclusters + 1) * sizeof(unsigned)) == cudaSuccess;
+    if (!ok) {
+        hb_ens_destroy(e);
+        return HB_ERR_CUDA;
+    }
+    EnsLaunch &L = e->L;
+    L.jp = e->d_jp;
+    L.dt = e->d_dt;
+    L.force = e->d_force;
+    L.partial = e->d_partial;
+    L.ilist = e->d_ilist;
+    L.ccnt = e->d_ccnt;
+    L.tile_base = e->d_tile_base;
+    L.counter = e->d_counter;
+    L.cl = e->d_cl;
+    L.slot_cluster = e->d_slot_cluster;
+    L.s = e->d_s;
+    L.err = e->d_err;
+    L.nslot = e->nslot;
+    L.nclusters = nclusters;
+    L.nsm = e->nsm;
+    L.partial_cap = e->partial_cap;
+    int smem = 0, per_sm = 0;
+    cudaError_t ce;
+    switch (order * 2 + (precision == HB_MIXED)) {
+    case 8: ce = ens_setup<4, false>(&smem, &per_sm); break;
+    case 9: ce = ens_setup<4, true>(&smem, &per_sm); break;
+    case 12: ce = ens_setup<6, false>(&smem, &per_sm); break;
+    case 13: ce = ens_setup<6, true>(&smem, &per_sm); break;
+    case 16: ce = ens_setup<8, false>(&smem, &per_sm); break;
+    default: ce = ens_setup<8, true>(&smem, &per_sm); break;
+    }
+    if (ce != cudaSuccess) {
+        hb_ens_destroy(e);
+        return HB_ERR_CUDA;
+    }
+    L.smem = smem;
+    L.items_grid = e->nsm * std::max(1, per_sm);
+    L.target_items = 2 * L.items_grid;
+    *out = e;
+    return HB_OK;
+}
+
+const char *hb_ens_last_error(const hb_ens *e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int hb_ens_cluster_offset(const hb_ens *e, int c)
+{
+    return (e && c >= 0 && c < e->nclusters) ? e->cl[c].off : -1;
+}
+
+int hb_ens_set_cluster(hb_ens *e, int c, const double *records, double eps2)
+{
+    if (!e || c < 0 || c >= e->nclusters || !records || !(eps2 >= 0.0)) return HB_ERR_INVALID;
+    e->cl[c].eps2 = eps2;
+    cudaError_t ce = cudaMemcpyAsync(e->d_jp + (size_t)e->cl[c].off * e->R, records,
+                                     sizeof(double) * (size_t)e->cl[c].n * e->R,
+                                     cudaMemcpyHostToDevice, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? HB_OK : ens_fail(e, HB_ERR_CUDA, "hb_ens_set_cluster", ce);
+}
+
+int hb_ens_get_cluster(hb_ens *e, int c, double *records, double *dt)
+{
+    if (!e || c < 0 || c >= e->nclusters || !records) return HB_ERR_INVALID;
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpy(records, e->d_jp + (size_t)e->cl[c].off * e->R,
+                        sizeof(double) * (size_t)e->cl[c].n * e->R, cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess && dt)
+        ce = cudaMemcpy(dt, e->d_dt + e->cl[c].off, sizeof(double) * e->cl[c].n, cudaMemcpyDeviceToHost);
+    return ce == cudaSuccess ? HB_OK : ens_fail(e, HB_ERR_CUDA, "hb_ens_get_cluster", ce);
+}
+
+int hb_ens_init(hb_ens *e, double tsys, double eta, double eta_s, double dtmax)
+{
+    if (!e) return HB_ERR_INVALID;
+    if (!(eta > 0.0) || !(eta_s > 0.0) || !(dtmax > 0.0) ||
+        std::log2(dtmax) != std::floor(std::log2(dtmax)) || !(tsys >= 0.0))
+        return ens_fail(e, HB_ERR_INVALID, "hb_ens_init: eta, eta_s > 0, dtmax a power of two");
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "sync", ce);
+    if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
+    if (e->graph) { cudaGraphDestroy(e->graph); e->graph = nullptr; }
+    e->ready = false;
+    // tlast = tsys, derivatives zero, for every real slot (device copy)
+    std::vector<double> rec;
+    for (int c = 0; c < e->nclusters; ++c) {
+        const Cluster &k = e->cl[c];
+        rec.resize((size_t)k.n * e->R);
+        ce = cudaMemcpy(rec.data(), e->d_jp + (size_t)k.off * e->R, rec.size() * sizeof(double),
+                        cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "init read", ce);
+        for (int i = 0; i < k.n; ++i) {
+            double *r = rec.data() + (size_t)i * e->R;
+            r[7] = tsys;
+            std::memset(r + 8, 0, sizeof(double) * (e->R - 8));
+        }
+        ce = cudaMemcpy(e->d_jp + (size_t)k.off * e->R, rec.data(), rec.size() * sizeof(double),
+                        cudaMemcpyHostToDevice);
+        if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "init write", ce);
+    }
+    ce = cudaMemcpy(e->d_cl, e->cl.data(), e->cl.size() * sizeof(Cluster), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "cluster table", ce);
+    EnsSched &s = *e->h_s;
+    std::memset(&s, 0, sizeof(EnsSched));
+    s.tnext_bits = kInf;
+    s.tsys = tsys;
+    s.tend = tsys;
+    s.tnext = tsys;       // the init force is evaluated at tsys
+    s.etapow = std::pow(eta, 2.0 * (e->order - 3));
+    s.dtmax = dtmax;
+    const bool m = e->precision == HB_MIXED;
+    const int passes = e->order > 4 ? 2 : 1;
+    for (int p = 0; p < passes && ce == cudaSuccess; ++p) {
+        switch (e->order) {
+        case 4: ce = ens_force_all<4>(e->L, m, p == passes - 1, eta_s, e->stream); break;
+        case 6: ce = ens_force_all<6>(e->L, m, p == passes - 1, eta_s, e->stream); break;
+        default: ce = ens_force_all<8>(e->L, m, p == passes - 1, eta_s, e->stream); break;
+        }
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "init forces", ce);
+    if (*e->h_err || s.error) return ens_fail(e, HB_ERR_DEVICE_TIMEOUT, "a device-side wait gave up");
+    s.particle_steps = s.block_steps = 0;
+    s.interactions = 0.0;
+    s.tnext_bits = kInf;
+    ce = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "capture", ce);
+    cudaError_t le = cudaSuccess;
+    for (int k = 0; k < kEnsStepsPerGraph && le == cudaSuccess; ++k) le = dispatch_step(e);
+    cudaGraph_t g = nullptr;
+    ce = cudaStreamEndCapture(e->stream, &g);
+    if (le != cudaSuccess || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return ens_fail(e, HB_ERR_CUDA, "capturing the ensemble step graph",
+                        le != cudaSuccess ? le : ce);
+    }
+    e->graph = g;
+    ce = cudaGraphInstantiate(&e->exec, g, 0);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "instantiate", ce);
+    e->ready = true;
+    return HB_OK;
+}
+
+int hb_ens_run(hb_ens *e, double tend, long long max_block_steps)
+{
+    if (!e) return HB_ERR_INVALID;
+    if (!e->ready) return ens_fail(e, HB_ERR_STATE, "hb_ens_run before hb_ens_init");
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "sync", ce);
+    volatile EnsSched *s = e->h_s;
+    if (!(tend >= s->tsys)) return ens_fail(e, HB_ERR_INVALID, "tend is before tsys");
+    s->tend = tend;
+    long long last = s->block_steps;
+    const long long first = s->block_steps;
+    while (s->tsys < tend) {
+        if (max_block_steps > 0 && s->block_steps - first >= max_block_steps)
+            return ens_fail(e, HB_ERR_STATE, "block-step limit reached");
+        ce = cudaGraphLaunch(e->exec, e->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+        if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "graph launch", ce);
+        if (*e->h_err || s->error)
+            return ens_fail(e, s->error == 1 ? HB_ERR_STATE : HB_ERR_DEVICE_TIMEOUT,
+                            s->error == 1 ? "a timestep underflowed (< 2^-48)"
+                                          : "a device-side wait gave up");
+        if (s->block_steps == last && s->tsys < tend)
+            return ens_fail(e, HB_ERR_STATE, "ensemble integration stalled");
+        last = s->block_steps;
+    }
+    return HB_OK;
+}
+
+int hb_ens_stats(const hb_ens *e, long long *particle_steps, long long *block_steps, double *tsys,
+                 double *interactions)
+{
+    if (!e) return HB_ERR_INVALID;
+    const volatile EnsSched *s = e->h_s;
+    if (particle_steps) *particle_steps = s->particle_steps;
+    if (block_steps) *block_steps = s->block_steps;
+    if (tsys) *tsys = s->tsys;
+    if (interactions) *interactions = s->interactions;
+    return HB_OK;
+}
+
+int hb_ens_energy(hb_ens *e, double *kinetic, double *potential)
+{
+    if (!e || !kinetic || !potential) return HB_ERR_INVALID;
+    cudaError_t ce = cudaMemcpy(e->d_cl, e->cl.data(), e->cl.size() * sizeof(Cluster),
+                                cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) {
+        switch (e->order) {
+        case 4: ce = ens_energy<4>(e->L, e->d_pot, e->d_eout, e->stream); break;
+        case 6: ce = ens_energy<6>(e->L, e->d_pot, e->d_eout, e->stream); break;
+        default: ce = ens_energy<8>(e->L, e->d_pot, e->d_eout, e->stream); break;
+        }
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "energy", ce);
+    for (int c = 0; c < e->nclusters; ++c) {
+        kinetic[c] = e->h_eout[2 * c];
+        potential[c] = e->h_eout[2 * c + 1];
+    }
+    return HB_OK;
+}
+
+}  // extern "C"

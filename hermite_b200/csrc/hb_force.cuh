@@ -32,21 +32,76 @@ struct Layout {
                                              : Pred64<ORDER>::chunk_bytes;
 };
 
-template <int ORDER, bool MIXED, int NW, int NI, int WJ, int TCH>
+template <int ORDER, bool MIXED, int NW, int NI, int WJ, int TCH, bool FUSED = false>
 struct ForceShape {
     static constexpr int F = Frc<ORDER>::words;
     static constexpr int WI = NW / WJ;
     static constexpr int TI = WI * 32 * NI;         // i per CTA
     static constexpr int STG = 2;
     static constexpr int CB = Layout<ORDER, MIXED>::chunk_bytes;
-    static constexpr int tile_bytes = TCH * CB;
+    // two-pass: the ring holds predicted tiles; fused: the ring holds raw
+    // records and one predicted tile sits after it
+    static constexpr int tile_bytes = FUSED ? TCH * 32 * Rec<ORDER>::bytes : TCH * CB;
     static constexpr int ring_bytes = STG * tile_bytes;
+    static constexpr int ptile_bytes = FUSED ? TCH * CB : 0;
     static constexpr int red_bytes = (WJ - 1) * WI * NI * F * 32 * 8;
-    static constexpr int body_bytes = ring_bytes > red_bytes ? ring_bytes : red_bytes;
+    static constexpr int work_bytes = ring_bytes + ptile_bytes;
+    static constexpr int body_bytes = work_bytes > red_bytes ? work_bytes : red_bytes;
     static constexpr int smem_bytes = body_bytes + 64;   // + mbarriers
     static_assert(NW % WJ == 0, "WJ must divide NW");
     static_assert(256 % TI == 0, "i-tile must divide the slot padding");
+    static_assert(!FUSED || TI <= TCH * 32, "fused: the i-tile must fit one raw stage");
 };
+
+// Predicts nslot consecutive records (raw, AoS) to tsys into the predicted
+// AoSoA32 layout at `out` (FP64 or hi/lo mixed), slots >= n as padding.
+// One out-of-line copy serves both the i- and the j-particles of the fused
+// kernel, so a particle's two predicted states are bit-identical and its
+// self term stays exactly zero.
+template <int ORDER, bool MIXED>
+__device__ __noinline__ void predict_tile(const double *raw, int nslot, int slot0, int n,
+                                          double tsys, void *out)
+{
+    constexpr int R = Rec<ORDER>::words;
+    for (int q = threadIdx.x; q < nslot; q += blockDim.x) {
+        double x[3], v[3], a[3] = {0, 0, 0}, jk[3] = {0, 0, 0}, m;
+        const int slot = slot0 + q;
+        if (slot < n) {
+            const double *r = raw + (size_t)q * R;
+            predict_slot<ORDER>(r, tsys, x, v, a, jk);
+            m = r[3];
+        } else {
+            for (int k = 0; k < 3; ++k) { x[k] = pad_position(slot, k); v[k] = 0.0; }
+            m = 0.0;
+        }
+        const int ci = q >> 5, lane = q & 31;
+        if constexpr (MIXED) {
+            constexpr int NC = PredMx<ORDER>::ncomp;
+            float *c = static_cast<float *>(out) + ci * NC * 32 + lane;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float hi = __double2float_rn(x[k]);
+                c[(PMX_XH + k) * 32] = hi;
+                c[(PMX_XL + k) * 32] = __double2float_rn(x[k] - (double)hi);
+                c[(PMX_V + k) * 32] = __double2float_rn(v[k]);
+                if constexpr (ORDER >= 6) c[(PMX_A + k) * 32] = __double2float_rn(a[k]);
+                if constexpr (ORDER == 8) c[(PMX_J + k) * 32] = __double2float_rn(jk[k]);
+            }
+            c[PMX_M * 32] = __double2float_rn(m);
+        } else {
+            constexpr int NC = Pred64<ORDER>::ncomp;
+            double *c = static_cast<double *>(out) + ci * NC * 32 + lane;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                c[(P64_X + k) * 32] = x[k];
+                c[(P64_V + k) * 32] = v[k];
+                if constexpr (ORDER >= 6) c[(P64_A + k) * 32] = a[k];
+                if constexpr (ORDER == 8) c[(P64_J + k) * 32] = jk[k];
+            }
+            c[P64_M * 32] = m;
+        }
+    }
+}
 
 // Loads the i-particles of lane `lane` in chunk `ci` from the predicted array.
 template <int ORDER>
@@ -82,11 +137,26 @@ __device__ __forceinline__ void load_i_mixed(const float *pred, int ci, int lane
     }
 }
 
+// Independent accumulator banks per i-particle in the chunk loops: with 2,
+// consecutive j (or j pairs) accumulate into different registers, so their
+// multiply-add chains do not serialise; the banks are added per chunk.
+#ifndef HB_ACC_BANKS
+#define HB_ACC_BANKS 1
+#endif
+
 // One 32-slot j chunk (in shared memory) against this thread's NI i-particles.
 template <int ORDER, int NI>
 __device__ __forceinline__ void chunk64(const double *cp, const Body64 (&I)[NI],
                                         double eps2, double (&f)[NI][Frc<ORDER>::words])
 {
+#if HB_ACC_BANKS == 2
+    constexpr int F = Frc<ORDER>::words;
+    double g[NI][F];
+#pragma unroll
+    for (int n = 0; n < NI; ++n)
+#pragma unroll
+        for (int c = 0; c < F; ++c) g[n][c] = 0.0;
+#endif
 #pragma unroll 2
     for (int jl = 0; jl < 32; jl += 2) {
         Body64 J0, J1;
@@ -106,9 +176,19 @@ __device__ __forceinline__ void chunk64(const double *cp, const Body64 (&I)[NI],
 #pragma unroll
         for (int n = 0; n < NI; ++n) {
             interact64<ORDER>(I[n], J0, eps2, f[n]);
+#if HB_ACC_BANKS == 2
+            interact64<ORDER>(I[n], J1, eps2, g[n]);
+#else
             interact64<ORDER>(I[n], J1, eps2, f[n]);
+#endif
         }
     }
+#if HB_ACC_BANKS == 2
+#pragma unroll
+    for (int n = 0; n < NI; ++n)
+#pragma unroll
+        for (int c = 0; c < F; ++c) f[n][c] += g[n][c];
+#endif
 }
 
 template <int ORDER, int NI, bool REFINE>
@@ -121,6 +201,13 @@ __device__ __forceinline__ void chunk_mixed(const float *cp, const NegI32 (&I)[N
     for (int n = 0; n < NI; ++n)
 #pragma unroll
         for (int c = 0; c < FS; ++c) s[n][c] = make_float2(0.f, 0.f);
+#if HB_ACC_BANKS == 2
+    float2 s2[NI][FS];
+#pragma unroll
+    for (int n = 0; n < NI; ++n)
+#pragma unroll
+        for (int c = 0; c < FS; ++c) s2[n][c] = make_float2(0.f, 0.f);
+#endif
 
 #pragma unroll 2
     for (int jl = 0; jl < 32; jl += 2) {
@@ -137,7 +224,11 @@ __device__ __forceinline__ void chunk_mixed(const float *cp, const NegI32 (&I)[N
 #pragma unroll
         for (int n = 0; n < NI; ++n) {
             float2 crk[3];
+#if HB_ACC_BANKS == 2
+            interact_mixed<ORDER, REFINE>(I[n], J, eps2, (jl & 2) ? s2[n] : s[n], crk);
+#else
             interact_mixed<ORDER, REFINE>(I[n], J, eps2, s[n], crk);
+#endif
             if constexpr (ORDER == 8) {
                 // crackle: FP64 accumulation of every pair term
 #pragma unroll
@@ -146,21 +237,36 @@ __device__ __forceinline__ void chunk_mixed(const float *cp, const NegI32 (&I)[N
             }
         }
     }
-    // flush the FP32 partial sums (32 pairs each) into the FP64 accumulators
+    // flush the FP32 partial sums into the FP64 accumulators
 #pragma unroll
     for (int n = 0; n < NI; ++n)
 #pragma unroll
-        for (int c = 0; c < FS; ++c) f[n][c] += (double)s[n][c].x + (double)s[n][c].y;
+        for (int c = 0; c < FS; ++c) {
+            f[n][c] += (double)s[n][c].x + (double)s[n][c].y;
+#if HB_ACC_BANKS == 2
+            f[n][c] += (double)s2[n][c].x + (double)s2[n][c].y;
+#endif
+        }
 }
 
-template <int ORDER, bool MIXED, int NW, int NI, int WJ, int TCH, bool REFINE = true>
-__global__ void __launch_bounds__(NW * 32)
+// Mixed precision: one Newton step on the hardware rsqrt measured no more
+// accurate on B200 (acc error max 4.4e-7 vs 5.0e-7, median 5.5e-8 vs 2.0e-8
+// without it, 6th order N=262144) and 8% slower, so it is off by default.
+#ifndef HB_MIXED_REFINE
+#define HB_MIXED_REFINE 0
+#endif
+
+template <int ORDER, bool MIXED, int NW, int NI, int WJ, int TCH, int MINB, bool FUSED = false,
+          bool REFINE = (HB_MIXED_REFINE != 0)>
+__global__ void __launch_bounds__(NW * 32, MINB)
 force_kernel(ForceArgs a)
 {
-    using Sh = ForceShape<ORDER, MIXED, NW, NI, WJ, TCH>;
+    using Sh = ForceShape<ORDER, MIXED, NW, NI, WJ, TCH, FUSED>;
     constexpr int F = Sh::F, WI = Sh::WI, TI = Sh::TI, STG = Sh::STG, CB = Sh::CB;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::body_bytes);
+    unsigned char *ptile = smem + Sh::ring_bytes;          // fused only
+    constexpr int RB = Rec<ORDER>::bytes;
     __shared__ unsigned s_last;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -180,27 +286,61 @@ force_kernel(ForceArgs a)
 
     using IBody = typename std::conditional<MIXED, NegI32, Body64>::type;
     IBody I[NI];
-#pragma unroll
-    for (int n = 0; n < NI; ++n) {
-        if constexpr (MIXED) load_i_mixed<ORDER>(static_cast<const float *>(a.pred), ichunk0 + n, lane, I[n]);
-        else load_i64<ORDER>(static_cast<const double *>(a.pred), ichunk0 + n, lane, I[n]);
-    }
 
     if (tid == 0) {
 #pragma unroll
-        for (int st = 0; st < STG; ++st) mbar_init(&bar[st], 1);
+        for (int st = 0; st < STG + 1; ++st) mbar_init(&bar[st], 1);
         fence_mbar_init();
     }
     __syncthreads();
+
+    if constexpr (FUSED) {
+        // this CTA's i-records -> raw stage 0 -> predicted tile -> registers
+        if (tid == 0) {
+            const uint32_t bytes = (uint32_t)(TI * RB);
+            mbar_arrive_expect_tx(&bar[STG], bytes);
+            bulk_load(smem, a.jp + (size_t)blockIdx.x * TI * Rec<ORDER>::words, bytes, &bar[STG]);
+        }
+        const bool got = mbar_wait_bounded(&bar[STG], 0);
+        if (!__syncthreads_and(got)) {
+            if (tid == 0) {
+                raise_error(a.err, kErrWaitTimeout);
+                mbar_wait_bounded(&bar[STG], 0);
+            }
+            return;
+        }
+        predict_tile<ORDER, MIXED>(reinterpret_cast<const double *>(smem), TI, blockIdx.x * TI,
+                                   a.nbody, a.tsys, ptile);
+        __syncthreads();
+#pragma unroll
+        for (int n = 0; n < NI; ++n) {
+            if constexpr (MIXED) load_i_mixed<ORDER>(reinterpret_cast<const float *>(ptile), ig * NI + n, lane, I[n]);
+            else load_i64<ORDER>(reinterpret_cast<const double *>(ptile), ig * NI + n, lane, I[n]);
+        }
+        __syncthreads();
+    } else {
+#pragma unroll
+        for (int n = 0; n < NI; ++n) {
+            if constexpr (MIXED) load_i_mixed<ORDER>(static_cast<const float *>(a.pred), ichunk0 + n, lane, I[n]);
+            else load_i64<ORDER>(static_cast<const double *>(a.pred), ichunk0 + n, lane, I[n]);
+        }
+    }
 
     auto issue = [&](int t) {   // thread 0 only
         const int st = t % STG;
         const int cs = c0 + t * TCH;
         const int cnt = min(TCH, c1 - cs);
-        const uint32_t bytes = (uint32_t)(cnt * CB);
-        mbar_arrive_expect_tx(&bar[st], bytes);
-        bulk_load(smem + st * Sh::tile_bytes,
-                  static_cast<const unsigned char *>(a.pred) + (size_t)cs * CB, bytes, &bar[st]);
+        if constexpr (FUSED) {
+            const uint32_t bytes = (uint32_t)(cnt * 32 * RB);
+            mbar_arrive_expect_tx(&bar[st], bytes);
+            bulk_load(smem + st * Sh::tile_bytes, a.jp + (size_t)cs * 32 * Rec<ORDER>::words,
+                      bytes, &bar[st]);
+        } else {
+            const uint32_t bytes = (uint32_t)(cnt * CB);
+            mbar_arrive_expect_tx(&bar[st], bytes);
+            bulk_load(smem + st * Sh::tile_bytes,
+                      static_cast<const unsigned char *>(a.pred) + (size_t)cs * CB, bytes, &bar[st]);
+        }
     };
     if (tid == 0)
         for (int t = 0; t < STG && t < ntile; ++t) issue(t);
@@ -213,6 +353,13 @@ force_kernel(ForceArgs a)
         if (!__syncthreads_and(got)) { failed_at = t; break; }
         const int cnt = min(TCH, c1 - (c0 + t * TCH));
         const unsigned char *tile = smem + st * Sh::tile_bytes;
+        if constexpr (FUSED) {
+            predict_tile<ORDER, MIXED>(reinterpret_cast<const double *>(tile), cnt * 32,
+                                       (c0 + t * TCH) * 32, a.nbody, a.tsys, ptile);
+            __syncthreads();
+            if (tid == 0 && t + STG < ntile) issue(t + STG);   // the raw stage is free
+            tile = ptile;
+        }
         for (int q = jg; q < cnt; q += WJ) {
             if constexpr (MIXED)
                 chunk_mixed<ORDER, NI, REFINE>(reinterpret_cast<const float *>(tile + q * CB), I, eps2f, f);
@@ -220,7 +367,7 @@ force_kernel(ForceArgs a)
                 chunk64<ORDER, NI>(reinterpret_cast<const double *>(tile + q * CB), I, a.eps2, f);
         }
         __syncthreads();
-        if (tid == 0 && t + STG < ntile) issue(t + STG);
+        if (!FUSED && tid == 0 && t + STG < ntile) issue(t + STG);
     }
     if (failed_at >= 0) {
         // Leave no bulk copy writing into this CTA's shared memory after exit.

@@ -1,0 +1,408 @@
+// hb_integrator.cu -- block-timestep Hermite integration resident on the GPU.
+//
+// The reference integrates on the host: per block step NbodySystem finds the
+// next block time and the active set (calc_dtlim / count_nact over a
+// dt-sorted array, SRC/nbodysystem.h:652-690), calls the force calculator,
+// corrects the active particles and re-sorts them (:693-765).  Here the whole
+// step stays on the device, four kernels per step, replayed from a captured
+// CUDA graph (no host round trip per step):
+//   1. next block time  = min over slots of (tlast + dt)   (grid reduction)
+//   2. active set       = slots with tlast + dt == tnext    (compaction),
+//                         dtlim from tnext                  (calc_dtlim)
+//   3. force            = fused predict + force on the active set, work items
+//                         (i-tile, j-slice) sized on the device from nact
+//   4. corrector        = Particle::correct + quantised Aarseth dt
+// Slots are never re-sorted; the j summation order is the slot order.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "hermite_b200.h"
+#include "hb_common.cuh"
+#include "hb_corrector.cuh"
+#include "hb_force.cuh"
+#include "hb_internal.h"
+
+namespace hb {
+
+constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;   // +inf
+
+// ---------------------------------------------------------------------------
+template <int ORDER>
+__global__ void sched_min_kernel(const double *__restrict__ jp, const double *__restrict__ dt,
+                                 int n, Sched *s)
+{
+    constexpr int R = Rec<ORDER>::words;
+    double m = __longlong_as_double((long long)kInfBits);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = fmin(m, dt[i] + jp[(size_t)i * R + 7]);
+    for (int o = 16; o; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double wm[32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? wm[threadIdx.x] : __longlong_as_double((long long)kInfBits);
+        for (int o = 16; o; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) atomicMin(&s->tnext_bits, (unsigned long long)__double_as_longlong(m));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        s->nact = 0;
+        s->work = 0;
+    }
+}
+
+// Active set and dtlim.  Positive doubles order like their bit patterns.
+template <int ORDER>
+__global__ void sched_compact_kernel(const double *__restrict__ jp, const double *__restrict__ dt,
+                                     int n, Sched *s, int *__restrict__ ilist)
+{
+    constexpr int R = Rec<ORDER>::words;
+    const double tnext = __longlong_as_double((long long)s->tnext_bits);
+    const bool live = tnext <= s->tend && s->error == 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // calc_dtlim (SRC/nbodysystem.h:652-661): the largest power-of-two
+        // fraction of dtmax that tnext is a multiple of
+        double dtlim = s->dtmax, q = tnext / s->dtmax;
+        for (int k = 0; k < 64 && q != trunc(q); ++k) {
+            q *= 2.0;
+            dtlim *= 0.5;
+        }
+        s->tnext = tnext;
+        s->dtlim = dtlim;
+    }
+    if (!live) return;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const int i = base + threadIdx.x;
+        const bool act = i < n && dt[i] + jp[(size_t)i * R + 7] == tnext;
+        const unsigned ballot = __ballot_sync(0xffffffffu, act);
+        int off = 0;
+        if ((threadIdx.x & 31) == 0 && ballot) off = atomicAdd(&s->nact, __popc(ballot));
+        off = __shfl_sync(0xffffffffu, off, 0);
+        if (act) ilist[off + __popc(ballot & ((1u << (threadIdx.x & 31)) - 1u))] = i;
+    }
+}
+
+// Fused predict + force over work items (i-tile of 32 active slots, j-slice),
+// taken from a device counter by a grid sized once; one warp per quarter of
+// every j tile (the 32 i are shared by the CTA's 4 warps).
+struct ItemsArgs {
+    const double *jp;
+    const int *ilist;
+    Sched *s;
+    double *force;      // [nact][F], indexed by position in ilist
+    double *partial;    // [S][gx*32][F]
+    unsigned *counter;  // [gx]
+    int *err;
+    int n, nchunk;
+    size_t partial_cap;
+    int target_items;
+};
+
+template <int ORDER, bool MIXED>
+__global__ void __launch_bounds__(128)
+force_items_kernel(ItemsArgs a)
+{
+    constexpr int NW = 4, WJ = 4, TCH = 4, STG = 2, TI = 32;
+    constexpr int F = Frc<ORDER>::words, R = Rec<ORDER>::words, RB = Rec<ORDER>::bytes;
+    using Sh = ForceShape<ORDER, MIXED, NW, 1, WJ, TCH, true>;
+    constexpr int CB = Sh::CB;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::body_bytes);
+    unsigned char *ptile = smem + Sh::ring_bytes;
+    __shared__ int s_item;
+    __shared__ unsigned s_last;
+
+    const int nact = a.s->nact;
+    if (nact == 0) return;
+    const double tsys = a.s->tnext, eps2 = a.s->eps2;
+    const int tid = threadIdx.x, lane = tid & 31, jg = tid >> 5;
+    const int gx = (nact + TI - 1) / TI;
+    int S = (a.target_items + gx - 1) / gx;
+    S = max(1, min(S, max(1, a.nchunk / 8)));
+    while (S > 1 && (size_t)S * gx * TI * F > a.partial_cap) --S;
+    const int items = gx * S;
+    const size_t ispan = (size_t)gx * TI;
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    unsigned g = 0;   // tiles issued by this CTA so far (mbarrier phases)
+    const float2 eps2f = f2((float)eps2);
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(&a.s->work, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= items) break;
+        const int itile = item / S, sl = item % S;
+
+        // gather the 32 i-records of this tile and predict them
+        double *raw = reinterpret_cast<double *>(smem);
+        for (int w = tid; w < TI * R; w += NW * 32) {
+            const int q = w / R, k = itile * TI + q;
+            const int slot = a.ilist[k < nact ? k : nact - 1];
+            raw[w] = a.jp[(size_t)slot * R + (w - q * R)];
+        }
+        __syncthreads();
+        predict_tile<ORDER, MIXED>(raw, TI, 0, 0x7fffffff, tsys, ptile);
+        __syncthreads();
+        using IBody = typename std::conditional<MIXED, NegI32, Body64>::type;
+        IBody I[1];
+        if constexpr (MIXED) load_i_mixed<ORDER>(reinterpret_cast<const float *>(ptile), 0, lane, I[0]);
+        else load_i64<ORDER>(reinterpret_cast<const double *>(ptile), 0, lane, I[0]);
+        __syncthreads();
+
+        double f[1][F];
+#pragma unroll
+        for (int c = 0; c < F; ++c) f[0][c] = 0.0;
+        const int c0 = (int)(((long long)sl * a.nchunk) / S);
+        const int c1 = (int)(((long long)(sl + 1) * a.nchunk) / S);
+        const int ntile = (c1 - c0 + TCH - 1) / TCH;
+        auto issue = [&](int t) {
+            const unsigned gt = g + t;
+            const int st = gt % STG;
+            const int cs = c0 + t * TCH, cnt = min(TCH, c1 - cs);
+            const uint32_t bytes = (uint32_t)(cnt * 32 * RB);
+            mbar_arrive_expect_tx(&bar[st], bytes);
+            bulk_load(smem + st * Sh::tile_bytes, a.jp + (size_t)cs * 32 * R, bytes, &bar[st]);
+        };
+        if (tid == 0)
+            for (int t = 0; t < STG && t < ntile; ++t) issue(t);
+        int failed_at = -1;
+        for (int t = 0; t < ntile; ++t) {
+            const unsigned gt = g + t;
+            const int st = gt % STG;
+            const bool got = mbar_wait_bounded(&bar[st], (gt / STG) & 1u);
+            if (!__syncthreads_and(got)) { failed_at = t; break; }
+            const int cnt = min(TCH, c1 - (c0 + t * TCH));
+            predict_tile<ORDER, MIXED>(reinterpret_cast<const double *>(smem + st * Sh::tile_bytes),
+                                       cnt * 32, (c0 + t * TCH) * 32, a.n, tsys, ptile);
+            __syncthreads();
+            if (tid == 0 && t + STG < ntile) issue(t + STG);
+            for (int q = jg; q < cnt; q += WJ) {
+                if constexpr (MIXED)
+                    chunk_mixed<ORDER, 1, (HB_MIXED_REFINE != 0)>(reinterpret_cast<const float *>(ptile + q * CB), I, eps2f, f);
+                else
+                    chunk64<ORDER, 1>(reinterpret_cast<const double *>(ptile + q * CB), I, eps2, f);
+            }
+            __syncthreads();
+        }
+        if (failed_at >= 0) {
+            if (tid == 0) {
+                raise_error(a.err, kErrWaitTimeout);
+                for (int t = failed_at; t < ntile && t < failed_at + STG; ++t)
+                    mbar_wait_bounded(&bar[(g + t) % STG], ((g + t) / STG) & 1u);
+            }
+            a.s->error = 2;
+            return;
+        }
+        g += ntile;
+
+        // the 4 warps' j quarters, in warp order
+        double *red = reinterpret_cast<double *>(smem);
+        if (jg > 0)
+#pragma unroll
+            for (int c = 0; c < F; ++c) red[((jg - 1) * F + c) * 32 + lane] = f[0][c];
+        __syncthreads();
+        const int k = itile * TI + lane;
+        if (jg == 0) {
+            for (int w = 1; w < WJ; ++w)
+#pragma unroll
+                for (int c = 0; c < F; ++c) f[0][c] += red[((w - 1) * F + c) * 32 + lane];
+            if (S == 1) {
+                if (k < nact)
+#pragma unroll
+                    for (int c = 0; c < F; ++c) a.force[(size_t)k * F + c] = f[0][c];
+            } else {
+#pragma unroll
+                for (int c = 0; c < F; ++c) a.partial[((size_t)sl * ispan + k) * F + c] = f[0][c];
+            }
+        }
+        if (S > 1) {
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) s_last = (atomicAdd(&a.counter[itile], 1u) == (unsigned)(S - 1));
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                const int V = min(TI, nact - itile * TI) * F;
+                const double *pbase = a.partial + (size_t)itile * TI * F;
+                for (int e = tid; e < V; e += NW * 32) {
+                    double sum = 0.0;
+                    for (int s2 = 0; s2 < S; ++s2) sum += __ldcg(pbase + (size_t)s2 * ispan * F + e);
+                    a.force[(size_t)itile * TI * F + e] = sum;
+                }
+                if (tid == 0) a.counter[itile] = 0u;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int ORDER>
+__global__ void correct_kernel(double *__restrict__ jp, double *__restrict__ dt,
+                               const double *__restrict__ force, const int *__restrict__ ilist,
+                               Sched *s)
+{
+    constexpr int R = Rec<ORDER>::words, F = Frc<ORDER>::words;
+    const int nact = s->nact;
+    const double dtlim = s->dtlim, etapow = s->etapow;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nact; k += gridDim.x * blockDim.x) {
+        const int i = ilist[k];
+        const double dtn = correct_particle<ORDER>(jp + (size_t)i * R, force + (size_t)k * F, dt[i],
+                                                   etapow, dtlim);
+        if (!(dtn >= 0x1p-48)) s->error = 1;   // timestep underflow (or NaN)
+        dt[i] = dtn;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (nact > 0) {
+            s->tsys = s->tnext;
+            s->particle_steps += nact;
+            s->block_steps += 1;
+        }
+        s->tnext_bits = kInfBits;
+    }
+}
+
+// Initialisation: write the force of all slots into the records (assign_force)
+// and, on the last pass, the initial dt (init_dt).
+template <int ORDER>
+__global__ void assign_kernel(double *__restrict__ jp, double *__restrict__ dt,
+                              const double *__restrict__ force, int n, int set_dt, double eta_s,
+                              double dtmax)
+{
+    constexpr int R = Rec<ORDER>::words, F = Frc<ORDER>::words;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double *r = jp + (size_t)i * R;
+    const double *f = force + (size_t)i * F;
+    for (int c = 0; c < F; ++c) r[8 + c] = f[c];
+    if (set_dt) dt[i] = initial_dt<ORDER>(f, eta_s, dtmax);
+}
+
+// 0.5*sum m v^2 and 0.5*sum m phi, per-block partials then one block, in a
+// fixed order.
+template <int ORDER>
+__global__ void energy_partial_kernel(const double *__restrict__ jp, const double *__restrict__ pot,
+                                      int n, double *__restrict__ part)
+{
+    constexpr int R = Rec<ORDER>::words;
+    double ke = 0.0, pe = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double *r = jp + (size_t)i * R;
+        ke += r[3] * (r[4] * r[4] + r[5] * r[5] + r[6] * r[6]);
+        pe += r[3] * pot[i];
+    }
+    __shared__ double sk[256], sp[256];
+    sk[threadIdx.x] = ke;
+    sp[threadIdx.x] = pe;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o; o >>= 1) {
+        if (threadIdx.x < o) {
+            sk[threadIdx.x] += sk[threadIdx.x + o];
+            sp[threadIdx.x] += sp[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = sk[0];
+        part[2 * blockIdx.x + 1] = sp[0];
+    }
+}
+
+__global__ void energy_final_kernel(const double *part, int nblk, double *out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double ke = 0.0, pe = 0.0;
+        for (int b = 0; b < nblk; ++b) {
+            ke += part[2 * b];
+            pe += part[2 * b + 1];
+        }
+        out[0] = 0.5 * ke;
+        out[1] = 0.5 * pe;
+    }
+}
+
+constexpr int kEnergyBlocks = 256;
+
+template <int ORDER>
+static cudaError_t launch_step(const IntegratorLaunch &L, cudaStream_t s)
+{
+    const int nb = std::min((L.n + 255) / 256, L.nsm * 8);
+    sched_min_kernel<ORDER><<<nb, 256, 0, s>>>(L.jp, L.dt, L.n, L.sched);
+    sched_compact_kernel<ORDER><<<nb, 256, 0, s>>>(L.jp, L.dt, L.n, L.sched, L.ilist);
+    ItemsArgs a{L.jp, L.ilist, L.sched, L.force, L.partial, L.counter, L.err, L.n, L.nchunk,
+                L.partial_cap, L.target_items};
+    if (L.mixed)
+        force_items_kernel<ORDER, true><<<L.items_grid, 128, L.smem_mixed, s>>>(a);
+    else
+        force_items_kernel<ORDER, false><<<L.items_grid, 128, L.smem_fp64, s>>>(a);
+    correct_kernel<ORDER><<<std::max(1, std::min(nb, L.nsm * 4)), 256, 0, s>>>(L.jp, L.dt, L.force,
+                                                                              L.ilist, L.sched);
+    return cudaGetLastError();
+}
+
+cudaError_t integrator_step_launch(int order, const IntegratorLaunch &L, cudaStream_t s)
+{
+    switch (order) {
+    case 4: return launch_step<4>(L, s);
+    case 6: return launch_step<6>(L, s);
+    case 8: return launch_step<8>(L, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *grid_per_sm)
+{
+    const void *k = nullptr;
+    int sm = 0;
+#define HB_ITEMS(O, M)                                                                        \
+    k = (const void *)&force_items_kernel<O, M>;                                                \
+    sm = ForceShape<O, M, 4, 1, 4, 4, true>::smem_bytes;
+    switch (order * 2 + (mixed ? 1 : 0)) {
+    case 8: HB_ITEMS(4, false) break;
+    case 9: HB_ITEMS(4, true) break;
+    case 12: HB_ITEMS(6, false) break;
+    case 13: HB_ITEMS(6, true) break;
+    case 16: HB_ITEMS(8, false) break;
+    case 17: HB_ITEMS(8, true) break;
+    default: return cudaErrorInvalidValue;
+    }
+#undef HB_ITEMS
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    *smem = sm;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(grid_per_sm, k, 128, sm);
+}
+
+cudaError_t integrator_assign(int order, double *jp, double *dt, const double *force, int n,
+                              int set_dt, double eta_s, double dtmax, cudaStream_t s)
+{
+    const int g = (n + 127) / 128;
+    switch (order) {
+    case 4: assign_kernel<4><<<g, 128, 0, s>>>(jp, dt, force, n, set_dt, eta_s, dtmax); break;
+    case 6: assign_kernel<6><<<g, 128, 0, s>>>(jp, dt, force, n, set_dt, eta_s, dtmax); break;
+    case 8: assign_kernel<8><<<g, 128, 0, s>>>(jp, dt, force, n, set_dt, eta_s, dtmax); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t integrator_energy(int order, const double *jp, const double *pot, int n, double *part,
+                              double *out, cudaStream_t s)
+{
+    switch (order) {
+    case 4: energy_partial_kernel<4><<<kEnergyBlocks, 256, 0, s>>>(jp, pot, n, part); break;
+    case 6: energy_partial_kernel<6><<<kEnergyBlocks, 256, 0, s>>>(jp, pot, n, part); break;
+    case 8: energy_partial_kernel<8><<<kEnergyBlocks, 256, 0, s>>>(jp, pot, n, part); break;
+    default: return cudaErrorInvalidValue;
+    }
+    energy_final_kernel<<<1, 32, 0, s>>>(part, kEnergyBlocks, out);
+    return cudaGetLastError();
+}
+
+}  // namespace hb

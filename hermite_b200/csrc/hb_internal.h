@@ -13,6 +13,11 @@ struct ForceArgs {
     double *partial;       // [S][gridDim.x*TI][F]  (only when S > 1)
     unsigned *counter;     // [gridDim.x], zero between launches
     int *err;              // mapped host flag
+    // fused predict + force only: raw j-particle records and the time to
+    // predict them to (slots >= nbody are padding)
+    const double *jp;
+    double tsys;
+    int nbody;
 };
 
 // One compiled launch shape of the force kernel.
@@ -23,8 +28,42 @@ struct ForceVariant {
     int tch;       // 32-slot chunks per j tile
     int ti;        // i per CTA
     int smem;      // dynamic shared memory bytes
+    bool fused;    // predicts j (and i) from the raw records itself
     void (*kern)(ForceArgs);
 };
+
+// Device-resident block-step integration (hb_integrator.cu).
+struct Sched {
+    unsigned long long tnext_bits;   // min(tlast + dt) as the bits of a positive double
+    int nact;                        // active slots of the current step
+    int work;                        // next force work item
+    int error;                       // 1: a timestep underflowed, 2: a device wait gave up
+    int pad;
+    double tnext, dtlim, tsys, tend;
+    double eps2, etapow, dtmax;
+    long long particle_steps, block_steps;
+};
+
+struct IntegratorLaunch {
+    double *jp;          // records (the state)
+    double *dt;          // per-slot timestep
+    int *ilist;          // active slots
+    Sched *sched;
+    double *force, *partial;
+    unsigned *counter;
+    int *err;
+    int n, nchunk, nsm;
+    size_t partial_cap;
+    int target_items, items_grid, smem_fp64, smem_mixed;
+    bool mixed;
+};
+
+cudaError_t integrator_step_launch(int order, const IntegratorLaunch &L, cudaStream_t s);
+cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *blocks_per_sm);
+cudaError_t integrator_assign(int order, double *jp, double *dt, const double *force, int n,
+                              int set_dt, double eta_s, double dtmax, cudaStream_t s);
+cudaError_t integrator_energy(int order, const double *jp, const double *pot, int n, double *part,
+                              double *out, cudaStream_t s);
 
 int force_variant_count(int order, bool mixed);
 const ForceVariant *force_variant(int order, bool mixed, int v);

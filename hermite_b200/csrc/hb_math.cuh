@@ -138,9 +138,8 @@ struct JPair32 {                // two j-particles
     float2 xh[3], xl[3], m, v[3], a[3], jk[3];
 };
 
-// Reciprocal square root of both halves: hardware rsqrt, then (if REFINE)
-// one Newton step y <- y*(3/2 - x y^2/2), which takes the error from the
-// ~2 ulp of the hardware approximation to FP32 rounding level.
+// Reciprocal square root of both halves: hardware rsqrt (documented maximum
+// error 2 ulp), then, if REFINE, one Newton step y <- y*(3/2 - x y^2/2).
 template <bool REFINE>
 __device__ __forceinline__ float2 rsqrt2(float2 x)
 {

@@ -114,7 +114,9 @@ const char *hb_status_string(int status);
 int hb_set_stream(hb_ctx *ctx, void *cuda_stream);
 /* Upload pending set_jp slots now (the copy part of predict_all). */
 int hb_upload(hb_ctx *ctx);
-/* The kernel part of predict_all: predict every slot, no upload. */
+/* The kernel part of predict_all: predict every slot to tsys, no upload.
+ * The prediction runs with the next force launch (inside the fused force
+ * kernel, or as a predictor pass ahead of a two-pass one). */
 int hb_predict_all_device(hb_ctx *ctx, double tsys);
 /* The kernel part of calc_force_on_first_nact: results stay in HBM
  * (hb_device_forces), nothing is copied back, no synchronisation. */
@@ -137,6 +139,67 @@ int hb_force_variant_count(int order, int precision);
 /* Describe a variant: threads per CTA, i per thread, warps splitting j. */
 int hb_force_variant_info(int order, int precision, int variant,
                           int *threads, int *i_per_thread, int *j_warps);
+
+/* ---- device-resident block-step integration ------------------------------
+ * The reference runs the Hermite corrector and the block-timestep scheduler
+ * on the host (NbodySystem::init_step / integrate_one_block,
+ * SRC/nbodysystem.h:565-631,693-765; Particle::correct and init_dt,
+ * SRC/hermite{4,6,8}.h).  These entry points run the same algorithm on the
+ * device: next block time = min(tlast + dt), active set, dtlim, fused
+ * predict + force on the active set, corrector with the quantised Aarseth
+ * step, 32 block steps per replay of a captured CUDA graph, no host round
+ * trip per step.  Slots are not re-sorted.  The state is the context's
+ * j-particle records plus a per-slot dt. */
+
+/* init_step: the current records' pos, mass and vel (set with set_jp) at
+ * tlast = tsys with zero derivatives are the initial conditions; forces are
+ * evaluated (twice for order > 4, to bootstrap snap/crackle), written into
+ * the records, and the initial dt set from eta_s and dtmax (a power of two).
+ * etapow = eta^(2*(order-3)) as the reference's set_run_params. */
+int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double eta_s,
+                       double dtmax);
+/* Integrate block steps on the device until the system time reaches tend
+ * (a multiple of dtmax for a synchronised end state).  max_block_steps > 0
+ * bounds the number of block steps of this call (HB_ERR_STATE when reached,
+ * with the state consistent at the time reached); 0 = no bound. */
+int hb_integrator_run(hb_ctx *ctx, double tend, long long max_block_steps);
+/* Counters since hb_integrator_init: sum of nact over block steps, block
+ * steps, and the current system time. */
+int hb_integrator_stats(const hb_ctx *ctx, long long *particle_steps, long long *block_steps,
+                        double *tsys);
+/* Kinetic 0.5*sum m v^2 and potential 0.5*sum m phi of the records (the
+ * reference's calc_energy, SRC/nbodysystem.h:633-650). */
+int hb_energy(hb_ctx *ctx, double eps2, double *kinetic, double *potential);
+/* Copy count records (and, if dt_out, their timesteps) from the device. */
+int hb_get_records(hb_ctx *ctx, int addr0, int count, double *records_out, double *dt_out);
+
+/* ---- batched ensembles ---------------------------------------------------
+ * No reference counterpart (the reference integrates one system per
+ * process).  Many independent clusters (any sizes, softenings, masses)
+ * advanced together by one device-resident block-step loop over the union
+ * of their particles; each particle interacts only with its own cluster.
+ * All clusters share eta, eta_s and dtmax; each has its own eps2. */
+typedef struct hb_ens hb_ens;
+int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_ens **out);
+int hb_ens_destroy(hb_ens *ens);
+const char *hb_ens_last_error(const hb_ens *ens);
+/* Initial conditions of cluster c: sizes[c] j-particle records (pos, mass,
+ * vel used; tlast and derivatives are reset by hb_ens_init) and its eps2. */
+int hb_ens_set_cluster(hb_ens *ens, int c, const double *records, double eps2);
+/* Current records (and dt) of cluster c. */
+int hb_ens_get_cluster(hb_ens *ens, int c, double *records, double *dt_out);
+/* Slot offset of cluster c in the ensemble's record array. */
+int hb_ens_cluster_offset(const hb_ens *ens, int c);
+/* init_step for every cluster (bootstrap forces, initial dt). */
+int hb_ens_init(hb_ens *ens, double tsys, double eta, double eta_s, double dtmax);
+/* Integrate all clusters until tend (max_block_steps as hb_integrator_run). */
+int hb_ens_run(hb_ens *ens, double tend, long long max_block_steps);
+/* Sums over block steps since init: particle steps, block steps, the
+ * current time, and interactions (sum of nact_c * N_c). */
+int hb_ens_stats(const hb_ens *ens, long long *particle_steps, long long *block_steps,
+                 double *tsys, double *interactions);
+/* Per-cluster kinetic and potential energy (arrays of nclusters). */
+int hb_ens_energy(hb_ens *ens, double *kinetic, double *potential);
 
 /* Measured peak of the FP32 (precision = HB_MIXED) or FP64 (HB_FP64) FMA
  * pipe on the current device, in GFLOP/s (2 flops per FMA), from a

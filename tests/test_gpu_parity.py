@@ -63,7 +63,7 @@ def test_mixed_partial_nact(order, nact, oracle):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", list(range(18)))
 @pytest.mark.parametrize("jsplit", [1, 3, 16])
 def test_every_launch_shape(precision, variant, jsplit, oracle):
     _check(6, 2500, 700, precision, oracle, seed=11, variant=variant, jsplit=jsplit)
@@ -80,15 +80,41 @@ def test_potential(order, oracle):
     np.testing.assert_allclose(got, ref, rtol=1e-13, atol=0)
 
 
-def test_self_term_is_zero(oracle):
-    """One particle: the force on it is exactly zero in both precisions."""
-    rec = make_records(8, 1, seed=2)
-    for prec in ("fp64", "mixed"):
-        with Gravity(8, 1, prec) as g:
+@pytest.mark.parametrize("variant", [0, 2, 12, 13])   # two-pass and fused shapes
+def test_self_term_is_zero(variant):
+    """One particle: the force on it is exactly zero in both precisions (the
+    fused kernel predicts i and j separately; the two states must agree to
+    the bit)."""
+    for order in (4, 6, 8):
+        rec = make_records(order, 1, seed=2)
+        for prec in ("fp64", "mixed"):
+            with Gravity(order, 1, prec) as g:
+                g.set_force_shape(variant, 0)
+                g.set_jp_records(rec)
+                g.predict_all(0.0)
+                f = g.calc_force_on_first_nact(1, EPS2)
+            assert np.all(f == 0.0), (order, prec, variant)
+
+
+@pytest.mark.parametrize("order", [4, 6, 8])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_matches_two_pass(order, precision):
+    """The fused predict+force shapes and the two-pass shapes (predictor
+    kernel, then force) agree: to summation-order rounding in FP64, to the
+    mixed tolerance otherwise."""
+    n, nact = 3000, 777
+    rec = make_records(order, n, seed=13)
+    out = {}
+    for v in (0, 12):
+        with Gravity(order, n, precision) as g:
+            g.set_force_shape(v, 4)
             g.set_jp_records(rec)
             g.predict_all(0.0)
-            f = g.calc_force_on_first_nact(1, EPS2)
-        assert np.all(f == 0.0), prec
+            out[v] = g.calc_force_on_first_nact(nact, EPS2)
+    err = rel_err(out[12], out[0])
+    tol = [FP64_TOL] * 4 if precision == "fp64" else [MIXED_TOL[k] for k in range(4)]
+    for k in range(err.shape[1]):
+        assert err[:, k].max() <= tol[k], (k, err[:, k].max())
 
 
 def test_upload_contract(oracle):

@@ -1,0 +1,59 @@
+"""The device-resident integrator (corrector + block-step scheduler on the GPU).
+
+Known answer: from gen-plum N=1k/2k with the run parameters of
+RUN/inp.{4,6,8}th, the mean number of active particles per block step over
+t = 0..1 and 1..2 must equal the reference's published values
+(RUN/gpu-{4,6,8}th.log) -- the whole block-step sequence, i.e. every
+quantised timestep of every particle, is reproduced by the device corrector
+and scheduler.  Energy conservation is checked against the reference's
+own integrator on the same snapshot.
+"""
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from kat import ETA, GEN_PLUM, PUBLISHED_NACT, ROOT, input_text
+
+pytestmark = pytest.mark.gpu
+
+
+def _snapshot(tmp_path, nk):
+    if not GEN_PLUM.exists():
+        pytest.skip("gen-plum not built (needs the reference sources)")
+    subprocess.run([str(GEN_PLUM), str(nk)], cwd=tmp_path, check=True, capture_output=True)
+    from hermite_b200.ic import read_snapshot
+    return read_snapshot(tmp_path / f"pl{nk}k.dat")
+
+
+@pytest.mark.parametrize("order,nk", [(4, 1), (6, 1), (8, 1), (4, 2), (6, 2)])
+def test_device_integrator_nact_known_answer(order, nk, tmp_path):
+    from hermite_b200 import Gravity
+    from hermite_b200.ic import records
+    snap = _snapshot(tmp_path, nk)
+    n = snap.n
+    eps = 4.0 / n / 1.0                      # kt_for_eps 1.0 (set_thermal_eps)
+    eta, eta_s = ETA[order]
+    with Gravity(order, n, "fp64") as g:
+        g.set_jp_records(records(snap, order))
+        g.integrator_init(0.0, eps * eps, eta, eta_s, 1.0 / 16)
+        ke0, pe0 = g.energy(eps * eps)
+        g.integrator_run(1.0)
+        ps1, bs1, t1 = g.integrator_stats()
+        g.integrator_run(2.0)
+        ps2, bs2, t2 = g.integrator_stats()
+        ke, pe = g.energy(eps * eps)
+    assert t1 == 1.0 and t2 == 2.0
+    got = ("%e" % (ps1 / bs1), "%e" % ((ps2 - ps1) / (bs2 - bs1)))
+    assert got == PUBLISHED_NACT[(order, n)]
+    e0, e2 = ke0 + pe0, ke + pe
+    de = (e0 - e2) / e0                      # the reference's de_glo sign
+    ref_app = ROOT / "oracle" / "_ref" / f"avx2-{order}"
+    if ref_app.exists():
+        r = subprocess.run([str(ref_app)], input=input_text(order, f"pl{nk}k.dat"), cwd=tmp_path,
+                           capture_output=True, text=True, timeout=600)
+        ref_de = float(re.findall(r"de\(local/global\) : \S+ (\S+)", r.stderr)[-1])
+        assert abs(de) <= 2.0 * abs(ref_de) + 1e-13, (de, ref_de)
+    else:
+        assert abs(de) < 1e-4, de
