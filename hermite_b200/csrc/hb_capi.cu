@@ -66,7 +66,9 @@ struct hb_ctx {
     int variant_override = -1, jsplit_override = 0;
 
     // device-resident integration (hb_integrator_*)
-    Sched *h_sched = nullptr, *d_sched = nullptr;   // mapped pinned
+    Sched *h_sched = nullptr;       // host copy of the scheduler (set-up only)
+    Sched *d_sched = nullptr;       // device scheduler
+    IntStatus *h_status = nullptr, *d_status = nullptr;   // mapped pinned
     double *d_dt = nullptr;
     int *d_ilist = nullptr;
     double *d_epart = nullptr, *h_eout = nullptr, *d_eout = nullptr;
@@ -314,7 +316,9 @@ int hb_destroy(hb_ctx *ctx)
     cudaFree(ctx->d_counter);
     if (ctx->int_exec) cudaGraphExecDestroy(ctx->int_exec);
     if (ctx->int_graph) cudaGraphDestroy(ctx->int_graph);
-    cudaFreeHost(ctx->h_sched);
+    delete ctx->h_sched;
+    cudaFree(ctx->d_sched);
+    cudaFreeHost(ctx->h_status);
     cudaFreeHost(ctx->h_eout);
     cudaFree(ctx->d_dt);
     cudaFree(ctx->d_ilist);
@@ -583,8 +587,9 @@ int integrator_alloc(hb_ctx *ctx)
 {
     if (ctx->h_sched) return HB_OK;
     const size_t np = ctx->npad;
-    bool ok = cudaHostAlloc((void **)&ctx->h_sched, sizeof(Sched), cudaHostAllocMapped) == cudaSuccess &&
-              cudaHostGetDevicePointer((void **)&ctx->d_sched, ctx->h_sched, 0) == cudaSuccess &&
+    bool ok = cudaMalloc((void **)&ctx->d_sched, sizeof(Sched)) == cudaSuccess &&
+              cudaHostAlloc((void **)&ctx->h_status, sizeof(IntStatus), cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer((void **)&ctx->d_status, ctx->h_status, 0) == cudaSuccess &&
               cudaHostAlloc((void **)&ctx->h_eout, 2 * sizeof(double), cudaHostAllocMapped) == cudaSuccess &&
               cudaHostGetDevicePointer((void **)&ctx->d_eout, ctx->h_eout, 0) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_dt, np * sizeof(double)) == cudaSuccess &&
@@ -594,6 +599,7 @@ int integrator_alloc(hb_ctx *ctx)
         cudaGetLastError();
         return fail(ctx, HB_ERR_ALLOC, "integrator buffers could not be allocated");
     }
+    ctx->h_sched = new Sched;
     return HB_OK;
 }
 }  // namespace
@@ -644,6 +650,10 @@ int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double
     sc.eps2 = eps2;
     sc.etapow = std::pow(eta, 2.0 * (ctx->order - 3));   // set_run_params, SRC/nbodysystem.h:472
     sc.dtmax = dtmax;
+    sc.status = ctx->d_status;
+    std::memset(ctx->h_status, 0, sizeof(IntStatus));
+    ctx->h_status->tsys = tsys;
+    HB_CK(cudaMemcpy(ctx->d_sched, &sc, sizeof(Sched), cudaMemcpyHostToDevice));
 
     IntegratorLaunch L;
     L.jp = ctx->d_jp;
@@ -690,25 +700,25 @@ int hb_integrator_run(hb_ctx *ctx, double tend, long long max_block_steps)
     if (!ctx->int_ready) return fail(ctx, HB_ERR_STATE, "hb_integrator_run before hb_integrator_init");
     int s = sync_stream(ctx);
     if (s != HB_OK) return s;
-    volatile Sched *sc = ctx->h_sched;
-    if (!(tend >= sc->tsys)) return fail(ctx, HB_ERR_INVALID, "tend %g is before tsys %g", tend, sc->tsys);
-    sc->tend = tend;
-    long long last_steps = sc->block_steps;
-    const long long first_steps = sc->block_steps;
-    for (long long launch = 0; sc->tsys < tend; ++launch) {
-        if (max_block_steps > 0 && sc->block_steps - first_steps >= max_block_steps)
+    volatile IntStatus *st = ctx->h_status;
+    if (!(tend >= st->tsys)) return fail(ctx, HB_ERR_INVALID, "tend %g is before tsys %g", tend, st->tsys);
+    HB_CK(cudaMemcpy(&ctx->d_sched->tend, &tend, sizeof(double), cudaMemcpyHostToDevice));
+    long long last_steps = st->block_steps;
+    const long long first_steps = st->block_steps;
+    while (st->tsys < tend) {
+        if (max_block_steps > 0 && st->block_steps - first_steps >= max_block_steps)
             return fail(ctx, HB_ERR_STATE, "block-step limit %lld reached at t = %.17g",
-                        max_block_steps, sc->tsys);
+                        max_block_steps, st->tsys);
         HB_CK(cudaGraphLaunch(ctx->int_exec, ctx->stream));
         ctx->launches += 4LL * kStepsPerGraph;
         s = sync_stream(ctx);
         if (s != HB_OK) return s;
-        if (sc->error)
-            return fail(ctx, sc->error == 2 ? HB_ERR_DEVICE_TIMEOUT : HB_ERR_STATE,
-                        sc->error == 2 ? "a device-side wait gave up" : "a timestep underflowed (< 2^-48)");
-        if (sc->block_steps == last_steps && sc->tsys < tend)
-            return fail(ctx, HB_ERR_STATE, "integration stalled at t = %.17g", sc->tsys);
-        last_steps = sc->block_steps;
+        if (st->error)
+            return fail(ctx, st->error == 2 ? HB_ERR_DEVICE_TIMEOUT : HB_ERR_STATE,
+                        st->error == 2 ? "a device-side wait gave up" : "a timestep underflowed (< 2^-48)");
+        if (st->block_steps == last_steps && st->tsys < tend)
+            return fail(ctx, HB_ERR_STATE, "integration stalled at t = %.17g", st->tsys);
+        last_steps = st->block_steps;
     }
     return HB_OK;
 }
@@ -716,11 +726,11 @@ int hb_integrator_run(hb_ctx *ctx, double tend, long long max_block_steps)
 int hb_integrator_stats(const hb_ctx *ctx, long long *particle_steps, long long *block_steps,
                         double *tsys)
 {
-    if (!ctx || !ctx->h_sched) return HB_ERR_INVALID;
-    const volatile Sched *sc = ctx->h_sched;
-    if (particle_steps) *particle_steps = sc->particle_steps;
-    if (block_steps) *block_steps = sc->block_steps;
-    if (tsys) *tsys = sc->tsys;
+    if (!ctx || !ctx->h_status) return HB_ERR_INVALID;
+    const volatile IntStatus *st = ctx->h_status;
+    if (particle_steps) *particle_steps = st->particle_steps;
+    if (block_steps) *block_steps = st->block_steps;
+    if (tsys) *tsys = st->tsys;
     return HB_OK;
 }
 

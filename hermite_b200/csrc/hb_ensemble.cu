@@ -42,6 +42,14 @@ struct Cluster {
     double eps2;
 };
 
+// host-visible mirror, written once per block step (mapped pinned memory)
+struct EnsStatus {
+    double tsys, interactions;
+    long long particle_steps, block_steps;
+    int error, pad;
+};
+
+// scheduler state in device memory (its atomics stay on the device)
 struct EnsSched {
     unsigned long long tnext_bits;
     int work, error, total_tiles, nact;
@@ -49,6 +57,7 @@ struct EnsSched {
     double etapow, dtmax;
     long long particle_steps, block_steps;
     double interactions;
+    EnsStatus *status;
 };
 
 struct EnsLaunch {
@@ -343,6 +352,12 @@ __global__ void ens_correct_kernel(EnsLaunch L)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (L.s->nact > 0) L.s->tsys = L.s->tnext;
         L.s->tnext_bits = kInf;
+        EnsStatus *st = L.s->status;
+        st->tsys = L.s->tsys;
+        st->interactions = L.s->interactions;
+        st->particle_steps = L.s->particle_steps;
+        st->block_steps = L.s->block_steps;
+        st->error = L.s->error;
     }
 }
 
@@ -474,7 +489,8 @@ struct hb_ens {
     int *d_ilist = nullptr, *d_ccnt = nullptr, *d_tile_base = nullptr, *d_slot_cluster = nullptr;
     unsigned *d_counter = nullptr;
     Cluster *d_cl = nullptr;
-    EnsSched *h_s = nullptr, *d_s = nullptr;
+    EnsSched *h_s = nullptr, *d_s = nullptr;       // host copy (set-up) / device
+    EnsStatus *h_st = nullptr, *d_st = nullptr;    // mapped
     int *h_err = nullptr, *d_err = nullptr;
     size_t partial_cap = 0;
     cudaGraph_t graph = nullptr;
@@ -530,7 +546,9 @@ int hb_ens_destroy(hb_ens *e)
     cudaFree(e->d_slot_cluster);
     cudaFree(e->d_counter);
     cudaFree(e->d_cl);
-    cudaFreeHost(e->h_s);
+    delete e->h_s;
+    cudaFree(e->d_s);
+    cudaFreeHost(e->h_st);
     cudaFreeHost(e->h_eout);
     cudaFreeHost(e->h_err);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -592,8 +610,9 @@ int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_
               cudaMalloc((void **)&e->d_slot_cluster, slot_cluster.size() * sizeof(int)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_counter, (ns / 32 + nclusters + 1) * sizeof(unsigned)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_cl, nclusters * sizeof(Cluster)) == cudaSuccess &&
-              cudaHostAlloc((void **)&e->h_s, sizeof(EnsSched), cudaHostAllocMapped) == cudaSuccess &&
-              cudaHostGetDevicePointer((void **)&e->d_s, e->h_s, 0) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_s, sizeof(EnsSched)) == cudaSuccess &&
+              cudaHostAlloc((void **)&e->h_st, sizeof(EnsStatus), cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer((void **)&e->d_st, e->h_st, 0) == cudaSuccess &&
               cudaHostAlloc((void **)&e->h_eout, 2 * nclusters * sizeof(double), cudaHostAllocMapped) == cudaSuccess &&
               cudaHostGetDevicePointer((void **)&e->d_eout, e->h_eout, 0) == cudaSuccess &&
               cudaHostAlloc((void **)&e->h_err, sizeof(int), cudaHostAllocMapped) == cudaSuccess &&
@@ -604,8 +623,11 @@ int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_
         return HB_ERR_ALLOC;
     }
     *e->h_err = 0;
+    e->h_s = new EnsSched;
     std::memset(e->h_s, 0, sizeof(EnsSched));
     e->h_s->tnext_bits = kInf;
+    e->h_s->status = e->d_st;
+    std::memset(e->h_st, 0, sizeof(EnsStatus));
     // inert padding everywhere until clusters are set
     std::vector<double> pad(ns * e->R, 0.0);
     std::vector<double> dt(ns, INFINITY);
@@ -726,6 +748,9 @@ int hb_ens_init(hb_ens *e, double tsys, double eta, double eta_s, double dtmax)
     s.tnext = tsys;       // the init force is evaluated at tsys
     s.etapow = std::pow(eta, 2.0 * (e->order - 3));
     s.dtmax = dtmax;
+    s.status = e->d_st;
+    ce = cudaMemcpy(e->d_s, &s, sizeof(EnsSched), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "scheduler upload", ce);
     const bool m = e->precision == HB_MIXED;
     const int passes = e->order > 4 ? 2 : 1;
     for (int p = 0; p < passes && ce == cudaSuccess; ++p) {
@@ -736,11 +761,17 @@ int hb_ens_init(hb_ens *e, double tsys, double eta, double eta_s, double dtmax)
         }
     }
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpy(&s, e->d_s, sizeof(EnsSched), cudaMemcpyDeviceToHost);
     if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "init forces", ce);
     if (*e->h_err || s.error) return ens_fail(e, HB_ERR_DEVICE_TIMEOUT, "a device-side wait gave up");
     s.particle_steps = s.block_steps = 0;
     s.interactions = 0.0;
     s.tnext_bits = kInf;
+    s.tsys = tsys;
+    ce = cudaMemcpy(e->d_s, &s, sizeof(EnsSched), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "scheduler upload", ce);
+    std::memset(e->h_st, 0, sizeof(EnsStatus));
+    e->h_st->tsys = tsys;
     ce = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
     if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "capture", ce);
     cudaError_t le = cudaSuccess;
@@ -765,24 +796,25 @@ int hb_ens_run(hb_ens *e, double tend, long long max_block_steps)
     if (!e->ready) return ens_fail(e, HB_ERR_STATE, "hb_ens_run before hb_ens_init");
     cudaError_t ce = cudaStreamSynchronize(e->stream);
     if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "sync", ce);
-    volatile EnsSched *s = e->h_s;
-    if (!(tend >= s->tsys)) return ens_fail(e, HB_ERR_INVALID, "tend is before tsys");
-    s->tend = tend;
-    long long last = s->block_steps;
-    const long long first = s->block_steps;
-    while (s->tsys < tend) {
-        if (max_block_steps > 0 && s->block_steps - first >= max_block_steps)
+    volatile EnsStatus *st = e->h_st;
+    if (!(tend >= st->tsys)) return ens_fail(e, HB_ERR_INVALID, "tend is before tsys");
+    ce = cudaMemcpy(&e->d_s->tend, &tend, sizeof(double), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "tend upload", ce);
+    long long last = st->block_steps;
+    const long long first = st->block_steps;
+    while (st->tsys < tend) {
+        if (max_block_steps > 0 && st->block_steps - first >= max_block_steps)
             return ens_fail(e, HB_ERR_STATE, "block-step limit reached");
         ce = cudaGraphLaunch(e->exec, e->stream);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
         if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "graph launch", ce);
-        if (*e->h_err || s->error)
-            return ens_fail(e, s->error == 1 ? HB_ERR_STATE : HB_ERR_DEVICE_TIMEOUT,
-                            s->error == 1 ? "a timestep underflowed (< 2^-48)"
-                                          : "a device-side wait gave up");
-        if (s->block_steps == last && s->tsys < tend)
+        if (*e->h_err || st->error)
+            return ens_fail(e, st->error == 1 ? HB_ERR_STATE : HB_ERR_DEVICE_TIMEOUT,
+                            st->error == 1 ? "a timestep underflowed (< 2^-48)"
+                                           : "a device-side wait gave up");
+        if (st->block_steps == last && st->tsys < tend)
             return ens_fail(e, HB_ERR_STATE, "ensemble integration stalled");
-        last = s->block_steps;
+        last = st->block_steps;
     }
     return HB_OK;
 }
@@ -791,7 +823,7 @@ int hb_ens_stats(const hb_ens *e, long long *particle_steps, long long *block_st
                  double *interactions)
 {
     if (!e) return HB_ERR_INVALID;
-    const volatile EnsSched *s = e->h_s;
+    const volatile EnsStatus *s = e->h_st;
     if (particle_steps) *particle_steps = s->particle_steps;
     if (block_steps) *block_steps = s->block_steps;
     if (tsys) *tsys = s->tsys;

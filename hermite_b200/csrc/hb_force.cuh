@@ -137,26 +137,11 @@ __device__ __forceinline__ void load_i_mixed(const float *pred, int ci, int lane
     }
 }
 
-// Independent accumulator banks per i-particle in the chunk loops: with 2,
-// consecutive j (or j pairs) accumulate into different registers, so their
-// multiply-add chains do not serialise; the banks are added per chunk.
-#ifndef HB_ACC_BANKS
-#define HB_ACC_BANKS 1
-#endif
-
 // One 32-slot j chunk (in shared memory) against this thread's NI i-particles.
 template <int ORDER, int NI>
 __device__ __forceinline__ void chunk64(const double *cp, const Body64 (&I)[NI],
                                         double eps2, double (&f)[NI][Frc<ORDER>::words])
 {
-#if HB_ACC_BANKS == 2
-    constexpr int F = Frc<ORDER>::words;
-    double g[NI][F];
-#pragma unroll
-    for (int n = 0; n < NI; ++n)
-#pragma unroll
-        for (int c = 0; c < F; ++c) g[n][c] = 0.0;
-#endif
 #pragma unroll 2
     for (int jl = 0; jl < 32; jl += 2) {
         Body64 J0, J1;
@@ -176,19 +161,9 @@ __device__ __forceinline__ void chunk64(const double *cp, const Body64 (&I)[NI],
 #pragma unroll
         for (int n = 0; n < NI; ++n) {
             interact64<ORDER>(I[n], J0, eps2, f[n]);
-#if HB_ACC_BANKS == 2
-            interact64<ORDER>(I[n], J1, eps2, g[n]);
-#else
             interact64<ORDER>(I[n], J1, eps2, f[n]);
-#endif
         }
     }
-#if HB_ACC_BANKS == 2
-#pragma unroll
-    for (int n = 0; n < NI; ++n)
-#pragma unroll
-        for (int c = 0; c < F; ++c) f[n][c] += g[n][c];
-#endif
 }
 
 template <int ORDER, int NI, bool REFINE>
@@ -201,13 +176,6 @@ __device__ __forceinline__ void chunk_mixed(const float *cp, const NegI32 (&I)[N
     for (int n = 0; n < NI; ++n)
 #pragma unroll
         for (int c = 0; c < FS; ++c) s[n][c] = make_float2(0.f, 0.f);
-#if HB_ACC_BANKS == 2
-    float2 s2[NI][FS];
-#pragma unroll
-    for (int n = 0; n < NI; ++n)
-#pragma unroll
-        for (int c = 0; c < FS; ++c) s2[n][c] = make_float2(0.f, 0.f);
-#endif
 
 #pragma unroll 2
     for (int jl = 0; jl < 32; jl += 2) {
@@ -224,11 +192,7 @@ __device__ __forceinline__ void chunk_mixed(const float *cp, const NegI32 (&I)[N
 #pragma unroll
         for (int n = 0; n < NI; ++n) {
             float2 crk[3];
-#if HB_ACC_BANKS == 2
-            interact_mixed<ORDER, REFINE>(I[n], J, eps2, (jl & 2) ? s2[n] : s[n], crk);
-#else
             interact_mixed<ORDER, REFINE>(I[n], J, eps2, s[n], crk);
-#endif
             if constexpr (ORDER == 8) {
                 // crackle: FP64 accumulation of every pair term
 #pragma unroll
@@ -241,12 +205,7 @@ __device__ __forceinline__ void chunk_mixed(const float *cp, const NegI32 (&I)[N
 #pragma unroll
     for (int n = 0; n < NI; ++n)
 #pragma unroll
-        for (int c = 0; c < FS; ++c) {
-            f[n][c] += (double)s[n][c].x + (double)s[n][c].y;
-#if HB_ACC_BANKS == 2
-            f[n][c] += (double)s2[n][c].x + (double)s2[n][c].y;
-#endif
-        }
+        for (int c = 0; c < FS; ++c) f[n][c] += (double)s[n][c].x + (double)s[n][c].y;
 }
 
 // Mixed precision: one Newton step on the hardware rsqrt measured no more

@@ -265,6 +265,11 @@ __global__ void correct_kernel(double *__restrict__ jp, double *__restrict__ dt,
             s->block_steps += 1;
         }
         s->tnext_bits = kInfBits;
+        IntStatus *st = s->status;
+        st->tsys = s->tsys;
+        st->particle_steps = s->particle_steps;
+        st->block_steps = s->block_steps;
+        st->error = s->error;
     }
 }
 

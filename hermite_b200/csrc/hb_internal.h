@@ -33,6 +33,16 @@ struct ForceVariant {
 };
 
 // Device-resident block-step integration (hb_integrator.cu).
+// What the host reads between graph replays; written once per block step by
+// one thread into mapped pinned memory (the scheduler itself stays in device
+// memory: its atomics must not cross the host link).
+struct IntStatus {
+    double tsys;
+    long long particle_steps, block_steps;
+    int error;
+    int pad;
+};
+
 struct Sched {
     unsigned long long tnext_bits;   // min(tlast + dt) as the bits of a positive double
     int nact;                        // active slots of the current step
@@ -42,6 +52,7 @@ struct Sched {
     double tnext, dtlim, tsys, tend;
     double eps2, etapow, dtmax;
     long long particle_steps, block_steps;
+    IntStatus *status;               // mapped mirror for the host
 };
 
 struct IntegratorLaunch {

@@ -21,8 +21,14 @@ namespace hb {
 //   (1 - h)^(-1/2) = 1 + h/2 + 3h^2/8 + O(h^3),   h = 1 - x*y0^2,
 // so y = y0*(1 + h/2 + 3h^2/8) has relative error ~ (5/16) h^3 < 2^-61,
 // i.e. it is correctly rounded up to the last bit or two of FP64.
+#ifndef HB_FP64_RSQRT_LIB
+#define HB_FP64_RSQRT_LIB 0
+#endif
 __device__ __forceinline__ double rsqrt_fp64(double x)
 {
+#if HB_FP64_RSQRT_LIB
+    return rsqrt(x);   // the CUDA math library's double-precision rsqrt
+#endif
     const double y0 = (double)rsqrtf((float)x);
     const double h = fma(-x * y0, y0, 1.0);
     return fma(y0 * h, fma(h, 0.375, 0.5), y0);
