@@ -16,20 +16,31 @@ namespace hb {
 
 // ---------------------------------------------------------------------------
 // Reciprocal square root in FP64.
-// Seed: the single-precision hardware rsqrt (relative error below 2^-21),
-// then one third-order correction from the binomial series
+// Seed y0: the double-precision approximate reciprocal square root
+// instruction (PTX rsqrt.approx.ftz.f64; no float conversions), then one
+// third-order correction from the binomial series
 //   (1 - h)^(-1/2) = 1 + h/2 + 3h^2/8 + O(h^3),   h = 1 - x*y0^2,
-// so y = y0*(1 + h/2 + 3h^2/8) has relative error ~ (5/16) h^3 < 2^-61,
-// i.e. it is correctly rounded up to the last bit or two of FP64.
-#ifndef HB_FP64_RSQRT_LIB
-#define HB_FP64_RSQRT_LIB 0
+// so y = y0*(1 + h/2 + 3h^2/8) has relative error ~ (5/16) h^3: below FP64
+// rounding for any seed error under 2^-18 (tests/test_fp64_rsqrt.py measures
+// the seed's error on the device).  HB_FP64_SEED=0 selects the
+// single-precision seed (double)rsqrtf((float)x) instead (two conversions).
+#ifndef HB_FP64_SEED
+#define HB_FP64_SEED 1
 #endif
+__device__ __forceinline__ double rsqrt_seed_fp64(double x)
+{
+#if HB_FP64_SEED == 1
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    return y;
+#else
+    return (double)rsqrtf((float)x);
+#endif
+}
+
 __device__ __forceinline__ double rsqrt_fp64(double x)
 {
-#if HB_FP64_RSQRT_LIB
-    return rsqrt(x);   // the CUDA math library's double-precision rsqrt
-#endif
-    const double y0 = (double)rsqrtf((float)x);
+    const double y0 = rsqrt_seed_fp64(x);
     const double h = fma(-x * y0, y0, 1.0);
     return fma(y0 * h, fma(h, 0.375, 0.5), y0);
 }
