@@ -42,6 +42,14 @@ struct Cluster {
     double eps2;
 };
 
+// Programmatic dependent launch (see hb_integrator.cu): schedule the next
+// kernel now, wait for the previous kernel's results.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // host-visible mirror, written once per block step (mapped pinned memory)
 struct EnsStatus {
     double tsys, interactions;
@@ -77,6 +85,7 @@ struct EnsLaunch {
 template <int ORDER>
 __global__ void ens_min_kernel(EnsLaunch L)
 {
+    pdl_enter();
     constexpr int R = Rec<ORDER>::words;
     double m = __longlong_as_double((long long)kInf);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.nslot; i += gridDim.x * blockDim.x)
@@ -99,6 +108,7 @@ __global__ void ens_min_kernel(EnsLaunch L)
 template <int ORDER>
 __global__ void ens_compact_kernel(EnsLaunch L)
 {
+    pdl_enter();
     constexpr int R = Rec<ORDER>::words;
     const double tnext = __longlong_as_double((long long)L.s->tnext_bits);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -126,6 +136,7 @@ __global__ void ens_compact_kernel(EnsLaunch L)
 // 2b. per-cluster i-tile offsets (one CTA)
 __global__ void ens_tiles_kernel(EnsLaunch L)
 {
+    pdl_enter();
     __shared__ int part[1024];
     const int per = (L.nclusters + blockDim.x - 1) / blockDim.x;
     const int c0 = threadIdx.x * per, c1 = min(L.nclusters, c0 + per);
@@ -175,6 +186,7 @@ template <int ORDER, bool MIXED>
 __global__ void __launch_bounds__(128)
 ens_force_kernel(EnsLaunch L)
 {
+    pdl_enter();
     constexpr int NW = 4, WJ = 4, TCH = 4, STG = 2, TI = 32;
     constexpr int F = Frc<ORDER>::words, R = Rec<ORDER>::words, RB = Rec<ORDER>::bytes;
     using Sh = ForceShape<ORDER, MIXED, NW, 1, WJ, TCH, true>;
@@ -330,6 +342,7 @@ ens_force_kernel(EnsLaunch L)
 template <int ORDER>
 __global__ void ens_correct_kernel(EnsLaunch L)
 {
+    pdl_enter();
     constexpr int R = Rec<ORDER>::words, F = Frc<ORDER>::words;
     const int T = L.s->total_tiles;
     const double dtlim = L.s->dtlim, etapow = L.s->etapow;
@@ -433,17 +446,34 @@ __global__ void ens_energy_kernel(EnsLaunch L, const double *pot, double *out)
     }
 }
 
+template <typename K>
+cudaError_t launch_pdl(K kern, int grid, int block, int smem, cudaStream_t s, const EnsLaunch &L)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, L);
+}
+
 template <int ORDER>
 cudaError_t ens_step(const EnsLaunch &L, bool mixed, cudaStream_t s)
 {
     const int nb = std::max(1, std::min((L.nslot + 127) / 128, L.nsm * 8));
-    ens_min_kernel<ORDER><<<nb, 256, 0, s>>>(L);
-    ens_compact_kernel<ORDER><<<nb, 128, 0, s>>>(L);
-    ens_tiles_kernel<<<1, 256, 0, s>>>(L);
-    if (mixed) ens_force_kernel<ORDER, true><<<L.items_grid, 128, L.smem, s>>>(L);
-    else ens_force_kernel<ORDER, false><<<L.items_grid, 128, L.smem, s>>>(L);
-    ens_correct_kernel<ORDER><<<L.nsm * 4, 128, 0, s>>>(L);
-    return cudaGetLastError();
+    cudaError_t e = launch_pdl(ens_min_kernel<ORDER>, nb, 256, 0, s, L);
+    if (e == cudaSuccess) e = launch_pdl(ens_compact_kernel<ORDER>, nb, 128, 0, s, L);
+    if (e == cudaSuccess) e = launch_pdl(ens_tiles_kernel, 1, 256, 0, s, L);
+    if (e == cudaSuccess)
+        e = mixed ? launch_pdl(ens_force_kernel<ORDER, true>, L.items_grid, 128, L.smem, s, L)
+                  : launch_pdl(ens_force_kernel<ORDER, false>, L.items_grid, 128, L.smem, s, L);
+    if (e == cudaSuccess) e = launch_pdl(ens_correct_kernel<ORDER>, L.nsm * 4, 128, 0, s, L);
+    return e;
 }
 
 template <int ORDER>

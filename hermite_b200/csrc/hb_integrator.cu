@@ -28,11 +28,22 @@ namespace hb {
 
 constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;   // +inf
 
+// Programmatic dependent launch: let the next kernel of the step be
+// scheduled now, then wait until the previous kernel's results are visible.
+// (The step's kernels are launched with programmatic stream serialisation;
+// without it both instructions are no-ops.)
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------
 template <int ORDER>
 __global__ void sched_min_kernel(const double *__restrict__ jp, const double *__restrict__ dt,
                                  int n, Sched *s)
 {
+    pdl_enter();
     constexpr int R = Rec<ORDER>::words;
     double m = __longlong_as_double((long long)kInfBits);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -57,6 +68,7 @@ template <int ORDER>
 __global__ void sched_compact_kernel(const double *__restrict__ jp, const double *__restrict__ dt,
                                      int n, Sched *s, int *__restrict__ ilist)
 {
+    pdl_enter();
     constexpr int R = Rec<ORDER>::words;
     const double tnext = __longlong_as_double((long long)s->tnext_bits);
     const bool live = tnext <= s->tend && s->error == 0;
@@ -103,6 +115,7 @@ template <int ORDER, bool MIXED>
 __global__ void __launch_bounds__(128)
 force_items_kernel(ItemsArgs a)
 {
+    pdl_enter();
     constexpr int NW = 4, WJ = 4, TCH = 4, STG = 2, TI = 32;
     constexpr int F = Frc<ORDER>::words, R = Rec<ORDER>::words, RB = Rec<ORDER>::bytes;
     using Sh = ForceShape<ORDER, MIXED, NW, 1, WJ, TCH, true>;
@@ -248,6 +261,7 @@ __global__ void correct_kernel(double *__restrict__ jp, double *__restrict__ dt,
                                const double *__restrict__ force, const int *__restrict__ ilist,
                                Sched *s)
 {
+    pdl_enter();
     constexpr int R = Rec<ORDER>::words, F = Frc<ORDER>::words;
     const int nact = s->nact;
     const double dtlim = s->dtlim, etapow = s->etapow;
@@ -334,21 +348,44 @@ __global__ void energy_final_kernel(const double *part, int nblk, double *out)
 
 constexpr int kEnergyBlocks = 256;
 
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kern)(KArgs...), int grid, int block, int smem, cudaStream_t s,
+                              Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <int ORDER>
 static cudaError_t launch_step(const IntegratorLaunch &L, cudaStream_t s)
 {
     const int nb = std::min((L.n + 255) / 256, L.nsm * 8);
-    sched_min_kernel<ORDER><<<nb, 256, 0, s>>>(L.jp, L.dt, L.n, L.sched);
-    sched_compact_kernel<ORDER><<<nb, 256, 0, s>>>(L.jp, L.dt, L.n, L.sched, L.ilist);
+    cudaError_t e = launch_pdl(sched_min_kernel<ORDER>, nb, 256, 0, s, (const double *)L.jp,
+                               (const double *)L.dt, L.n, L.sched);
+    if (e == cudaSuccess)
+        e = launch_pdl(sched_compact_kernel<ORDER>, nb, 256, 0, s, (const double *)L.jp,
+                       (const double *)L.dt, L.n, L.sched, L.ilist);
     ItemsArgs a{L.jp, L.ilist, L.sched, L.force, L.partial, L.counter, L.err, L.n, L.nchunk,
                 L.partial_cap, L.target_items};
-    if (L.mixed)
-        force_items_kernel<ORDER, true><<<L.items_grid, 128, L.smem_mixed, s>>>(a);
-    else
-        force_items_kernel<ORDER, false><<<L.items_grid, 128, L.smem_fp64, s>>>(a);
-    correct_kernel<ORDER><<<std::max(1, std::min(nb, L.nsm * 4)), 256, 0, s>>>(L.jp, L.dt, L.force,
-                                                                              L.ilist, L.sched);
-    return cudaGetLastError();
+    if (e == cudaSuccess) {
+        if (L.mixed)
+            e = launch_pdl(force_items_kernel<ORDER, true>, L.items_grid, 128, L.smem_mixed, s, a);
+        else
+            e = launch_pdl(force_items_kernel<ORDER, false>, L.items_grid, 128, L.smem_fp64, s, a);
+    }
+    if (e == cudaSuccess)
+        e = launch_pdl(correct_kernel<ORDER>, std::max(1, std::min(nb, L.nsm * 4)), 256, 0, s, L.jp,
+                       L.dt, (const double *)L.force, (const int *)L.ilist, L.sched);
+    return e;
 }
 
 cudaError_t integrator_step_launch(int order, const IntegratorLaunch &L, cudaStream_t s)
