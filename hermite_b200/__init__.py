@@ -46,10 +46,14 @@ EXPORTED_SYMBOLS = (
     "hb_synchronize", "hb_launch_count", "hb_set_force_shape", "hb_force_variant_count",
     "hb_force_variant_info", "hb_measure_fma_peak", "hb_force_predicted_noalloc",
     "hb_integrator_init", "hb_integrator_run", "hb_integrator_stats", "hb_energy",
+    "hb_integrator_set_engine", "hb_integrator_engine",
     "hb_get_records", "hb_ens_create", "hb_ens_destroy", "hb_ens_last_error",
     "hb_ens_set_cluster", "hb_ens_get_cluster", "hb_ens_cluster_offset", "hb_ens_init",
     "hb_ens_run", "hb_ens_stats", "hb_ens_energy",
 )
+
+
+ENGINES = {"auto": 0, "graph": 1, "team": 2}
 
 
 def record_words(order: int) -> int:
@@ -109,6 +113,8 @@ def load_library() -> ctypes.CDLL:
         "hb_force_predicted_noalloc": (I, [I, I, P, I, I, D, P, P]),
         "hb_integrator_init": (I, [P, D, D, D, D, D]),
         "hb_integrator_run": (I, [P, D, ctypes.c_longlong]),
+        "hb_integrator_set_engine": (I, [P, I, I]),
+        "hb_integrator_engine": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "hb_integrator_stats": (I, [P, ctypes.POINTER(ctypes.c_longlong),
                                     ctypes.POINTER(ctypes.c_longlong), dp]),
         "hb_energy": (I, [P, D, dp, dp]),
@@ -262,6 +268,19 @@ class Gravity:
     def integrator_run(self, tend: float, max_block_steps: int = 0):
         self._check(self._lib.hb_integrator_run(self._h, float(tend), int(max_block_steps)),
                      "integrator_run")
+
+    def set_engine(self, engine: str = "auto", team_ctas: int = 0):
+        """Integration engine: "auto", "graph" (multi-kernel, CUDA graph) or
+        "team" (one thread-block cluster, whole loop in one kernel)."""
+        self._check(self._lib.hb_integrator_set_engine(self._h, ENGINES[engine], int(team_ctas)),
+                    "set_engine")
+
+    def engine(self):
+        """(engine name, CTAs per team) that the next integrator_run uses."""
+        e, c = ctypes.c_int(), ctypes.c_int()
+        self._check(self._lib.hb_integrator_engine(self._h, ctypes.byref(e), ctypes.byref(c)),
+                    "engine")
+        return {v: k for k, v in ENGINES.items()}[e.value], c.value
 
     def integrator_stats(self):
         ps, bs, t = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()

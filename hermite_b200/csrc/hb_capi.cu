@@ -30,6 +30,8 @@ using namespace hb;
 
 namespace {
 constexpr int kMaxBody = 1 << 24;
+// HB_ENGINE_AUTO takes the team engine up to this many particles.
+constexpr int kTeamAutoMaxBody = 3072;
 constexpr int kNumVariants = 18;
 
 int rec_words(int order) { return 8 + 3 * (order - 2); }
@@ -75,6 +77,11 @@ struct hb_ctx {
     cudaGraph_t int_graph = nullptr;
     cudaGraphExec_t int_exec = nullptr;
     bool int_ready = false;
+    // team engine (hb_team.cu)
+    int engine = HB_ENGINE_AUTO, team_ctas = 0;
+    TeamSys *d_team_sys = nullptr;
+    TeamState *d_team_state = nullptr;
+    int *d_team_next = nullptr;
     int blocks_per_sm[2][kNumVariants] = {};
     bool smem_set[2][kNumVariants] = {};
     std::string err;
@@ -323,6 +330,9 @@ int hb_destroy(hb_ctx *ctx)
     cudaFree(ctx->d_dt);
     cudaFree(ctx->d_ilist);
     cudaFree(ctx->d_epart);
+    cudaFree(ctx->d_team_sys);
+    cudaFree(ctx->d_team_state);
+    cudaFree(ctx->d_team_next);
     if (ctx->ev_upload) cudaEventDestroy(ctx->ev_upload);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -594,7 +604,10 @@ int integrator_alloc(hb_ctx *ctx)
               cudaHostGetDevicePointer((void **)&ctx->d_eout, ctx->h_eout, 0) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_dt, np * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_ilist, np * sizeof(int)) == cudaSuccess &&
-              cudaMalloc((void **)&ctx->d_epart, 2 * kEnergyParts * sizeof(double)) == cudaSuccess;
+              cudaMalloc((void **)&ctx->d_epart, 2 * kEnergyParts * sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void **)&ctx->d_team_sys, sizeof(TeamSys)) == cudaSuccess &&
+              cudaMalloc((void **)&ctx->d_team_state, sizeof(TeamState)) == cudaSuccess &&
+              cudaMalloc((void **)&ctx->d_team_next, sizeof(int)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         return fail(ctx, HB_ERR_ALLOC, "integrator buffers could not be allocated");
@@ -654,6 +667,8 @@ int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double
     std::memset(ctx->h_status, 0, sizeof(IntStatus));
     ctx->h_status->tsys = tsys;
     HB_CK(cudaMemcpy(ctx->d_sched, &sc, sizeof(Sched), cudaMemcpyHostToDevice));
+    const TeamSys ts{0, ctx->nbody, 0, eps2};
+    HB_CK(cudaMemcpy(ctx->d_team_sys, &ts, sizeof(TeamSys), cudaMemcpyHostToDevice));
 
     IntegratorLaunch L;
     L.jp = ctx->d_jp;
@@ -694,6 +709,111 @@ int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double
     return HB_OK;
 }
 
+namespace {
+constexpr long long kTeamStepsPerLaunch = 1LL << 14;
+
+// The team size for one system of n slots: about kTeamChunksPerCta 32-slot
+// chunks per CTA, at most 16 CTAs (8 where the device cannot co-schedule a
+// 16-CTA cluster with this kernel's shared memory).
+constexpr int kTeamChunksPerCta = 2;
+
+int team_config_for(hb_ctx *ctx, int n, int want_ctas, TeamConfig *cfg)
+{
+    const int nch = (n + 31) / 32;
+    int ctas = want_ctas > 0 ? want_ctas
+                             : std::min(16, std::max(1, (nch + kTeamChunksPerCta - 1) / kTeamChunksPerCta));
+    for (;;) {
+        const cudaError_t e = team_setup(ctx->order, ctas, cfg);
+        if (e == cudaSuccess && cfg->max_teams >= 1) break;
+        cudaGetLastError();
+        if (want_ctas > 0 || ctas <= 8) return fail(ctx, HB_ERR_CUDA, "a team of %d CTAs cannot be scheduled", ctas);
+        ctas = 8;
+    }
+    if ((long long)((nch + ctas - 1) / ctas) * 32 > cfg->jl_cap)
+        return fail(ctx, HB_ERR_TOO_LARGE, "%d slots do not fit a team of %d CTAs (%d slots each)", n,
+                    ctas, cfg->jl_cap);
+    return HB_OK;
+}
+
+// The engine the next hb_integrator_run uses.
+int resolve_engine(hb_ctx *ctx, TeamConfig *cfg)
+{
+    if (ctx->engine == HB_ENGINE_GRAPH) return HB_ENGINE_GRAPH;
+    const bool fp64 = ctx->precision == HB_FP64;
+    if (ctx->engine == HB_ENGINE_TEAM) {
+        if (!fp64) return -fail(ctx, HB_ERR_INVALID, "the team engine integrates in FP64 only");
+        const int s = team_config_for(ctx, ctx->nbody, ctx->team_ctas, cfg);
+        return s == HB_OK ? HB_ENGINE_TEAM : -s;
+    }
+    if (!fp64 || ctx->nbody > kTeamAutoMaxBody) return HB_ENGINE_GRAPH;
+    return team_config_for(ctx, ctx->nbody, ctx->team_ctas, cfg) == HB_OK ? HB_ENGINE_TEAM
+                                                                          : HB_ENGINE_GRAPH;
+}
+
+int run_team(hb_ctx *ctx, const TeamConfig &cfg, double tend, long long max_block_steps)
+{
+    volatile IntStatus *st = ctx->h_status;
+    HB_CK(team_sched_sync(ctx->d_sched, ctx->d_team_state, true, ctx->stream));
+    TeamLaunch L;
+    L.jp = ctx->d_jp;
+    L.dt = ctx->d_dt;
+    L.sys = ctx->d_team_sys;
+    L.st = ctx->d_team_state;
+    L.next_sys = ctx->d_team_next;
+    L.nsys = 1;
+    L.ctas = cfg.ctas;
+    L.jl_cap = cfg.jl_cap;
+    L.smem = cfg.smem;
+    L.tend = tend;
+    L.etapow = ctx->h_sched->etapow;
+    L.dtmax = ctx->h_sched->dtmax;
+    const long long first_steps = st->block_steps;
+    long long last_steps = st->block_steps;
+    while (st->tsys < tend) {
+        long long budget = kTeamStepsPerLaunch;
+        if (max_block_steps > 0) {
+            const long long left = max_block_steps - (st->block_steps - first_steps);
+            if (left <= 0)
+                return fail(ctx, HB_ERR_STATE, "block-step limit %lld reached at t = %.17g",
+                            max_block_steps, st->tsys);
+            budget = std::min(budget, left);
+        }
+        L.max_steps = budget;
+        HB_CK(cudaMemsetAsync(ctx->d_team_next, 0, sizeof(int), ctx->stream));
+        HB_CK(team_launch(ctx->order, L, 1, ctx->stream));
+        HB_CK(team_sched_sync(ctx->d_sched, ctx->d_team_state, false, ctx->stream));
+        ctx->launches += 1;
+        const int s = sync_stream(ctx);
+        if (s != HB_OK) return s;
+        if (st->error) return fail(ctx, HB_ERR_STATE, "a timestep underflowed (< 2^-48)");
+        if (st->block_steps == last_steps && st->tsys < tend)
+            return fail(ctx, HB_ERR_STATE, "integration stalled at t = %.17g", st->tsys);
+        last_steps = st->block_steps;
+    }
+    return HB_OK;
+}
+}  // namespace
+
+int hb_integrator_set_engine(hb_ctx *ctx, int engine, int team_ctas)
+{
+    if (!ctx || engine < HB_ENGINE_AUTO || engine > HB_ENGINE_TEAM || team_ctas < 0 || team_ctas > 16)
+        return HB_ERR_INVALID;
+    ctx->engine = engine;
+    ctx->team_ctas = team_ctas;
+    return HB_OK;
+}
+
+int hb_integrator_engine(hb_ctx *ctx, int *engine, int *team_ctas)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    TeamConfig cfg{};
+    const int r = resolve_engine(ctx, &cfg);
+    if (r < 0) return -r;
+    if (engine) *engine = r;
+    if (team_ctas) *team_ctas = r == HB_ENGINE_TEAM ? cfg.ctas : 0;
+    return HB_OK;
+}
+
 int hb_integrator_run(hb_ctx *ctx, double tend, long long max_block_steps)
 {
     if (!ctx) return HB_ERR_INVALID;
@@ -703,6 +823,10 @@ int hb_integrator_run(hb_ctx *ctx, double tend, long long max_block_steps)
     volatile IntStatus *st = ctx->h_status;
     if (!(tend >= st->tsys)) return fail(ctx, HB_ERR_INVALID, "tend %g is before tsys %g", tend, st->tsys);
     HB_CK(cudaMemcpy(&ctx->d_sched->tend, &tend, sizeof(double), cudaMemcpyHostToDevice));
+    TeamConfig cfg{};
+    const int engine = resolve_engine(ctx, &cfg);
+    if (engine < 0) return -engine;
+    if (engine == HB_ENGINE_TEAM) return run_team(ctx, cfg, tend, max_block_steps);
     long long last_steps = st->block_steps;
     const long long first_steps = st->block_steps;
     while (st->tsys < tend) {

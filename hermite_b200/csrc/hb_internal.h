@@ -70,6 +70,42 @@ struct IntegratorLaunch {
 };
 
 cudaError_t integrator_step_launch(int order, const IntegratorLaunch &L, cudaStream_t s);
+
+// Team engine (hb_team.cu): one thread-block cluster of `ctas` CTAs runs the
+// whole block-step loop of one system at a time inside one kernel.
+constexpr int kTeamIMax = 256;              // active slots per force round
+constexpr int kTeamMaxSlotsPerCta = 2048;
+struct TeamSys {
+    long long off;     // first slot of the system in the record / dt arrays
+    int n, pad;
+    double eps2;
+};
+struct TeamState {     // per system, persistent across launches
+    double tsys;
+    long long particle_steps, block_steps;
+    double interactions;
+    int error, pad;
+};
+struct TeamConfig {
+    int ctas;          // CTAs per team (cluster size)
+    int jl_cap;        // slots per CTA that fit in shared memory
+    int smem;          // dynamic shared memory per CTA
+    int max_teams;     // co-resident teams on this device
+};
+struct TeamLaunch {
+    double *jp, *dt;
+    const TeamSys *sys;
+    TeamState *st;
+    int *next_sys;     // work counter, zero at launch
+    int nsys;
+    int ctas, jl_cap, smem;
+    double tend, etapow, dtmax;
+    long long max_steps;   // per system and launch
+};
+cudaError_t team_setup(int order, int ctas, TeamConfig *cfg);
+cudaError_t team_launch(int order, const TeamLaunch &L, int teams, cudaStream_t s);
+cudaError_t team_sched_sync(Sched *s, TeamState *st, bool to_team, cudaStream_t stream);
+
 cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *blocks_per_sm);
 cudaError_t integrator_assign(int order, double *jp, double *dt, const double *force, int n,
                               int set_dt, double eta_s, double dtmax, cudaStream_t s);

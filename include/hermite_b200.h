@@ -158,6 +158,22 @@ int hb_force_variant_info(int order, int precision, int variant,
  * etapow = eta^(2*(order-3)) as the reference's set_run_params. */
 int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double eta_s,
                        double dtmax);
+/* Engines for hb_integrator_run (same state, same algorithm):
+ *  HB_ENGINE_GRAPH  four kernels per block step over the whole GPU, 32 steps
+ *                   per replay of a CUDA graph (any N, FP64 or mixed);
+ *  HB_ENGINE_TEAM   one thread-block cluster of up to 16 CTAs runs the whole
+ *                   block-step loop in one kernel, three cluster barriers per
+ *                   step (FP64; N up to 16 x the slots one CTA holds in
+ *                   shared memory, about 16k);
+ *  HB_ENGINE_AUTO   the team engine for FP64 systems of up to 3072
+ *                   particles, else the graph engine (the default).
+ * team_ctas: CTAs per team (1..16), 0 = chosen from N. */
+enum { HB_ENGINE_AUTO = 0, HB_ENGINE_GRAPH = 1, HB_ENGINE_TEAM = 2 };
+int hb_integrator_set_engine(hb_ctx *ctx, int engine, int team_ctas);
+/* The engine (HB_ENGINE_GRAPH or HB_ENGINE_TEAM) and team size the next
+ * hb_integrator_run uses; HB_ERR_TOO_LARGE / HB_ERR_INVALID when a forced
+ * team engine cannot take this system. */
+int hb_integrator_engine(hb_ctx *ctx, int *engine, int *team_ctas);
 /* Integrate block steps on the device until the system time reaches tend
  * (a multiple of dtmax for a synchronised end state).  max_block_steps > 0
  * bounds the number of block steps of this call (HB_ERR_STATE when reached,

@@ -27,8 +27,9 @@ def _snapshot(tmp_path, nk):
     return read_snapshot(tmp_path / f"pl{nk}k.dat")
 
 
+@pytest.mark.parametrize("engine", ["graph", "team"])
 @pytest.mark.parametrize("order,nk", [(4, 1), (6, 1), (8, 1), (4, 2), (6, 2)])
-def test_device_integrator_nact_known_answer(order, nk, tmp_path):
+def test_device_integrator_nact_known_answer(order, nk, engine, tmp_path):
     from hermite_b200 import Gravity
     from hermite_b200.ic import records
     snap = _snapshot(tmp_path, nk)
@@ -36,6 +37,8 @@ def test_device_integrator_nact_known_answer(order, nk, tmp_path):
     eps = 4.0 / n / 1.0                      # kt_for_eps 1.0 (set_thermal_eps)
     eta, eta_s = ETA[order]
     with Gravity(order, n, "fp64") as g:
+        g.set_engine(engine)
+        assert g.engine()[0] == engine
         g.set_jp_records(records(snap, order))
         g.integrator_init(0.0, eps * eps, eta, eta_s, 1.0 / 16)
         ke0, pe0 = g.energy(eps * eps)
