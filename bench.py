@@ -335,6 +335,7 @@ def run_ours(args):
     integ = device_integrator_leg() if not args.skip_integrator else None
     ref_gpu = reference_gpu_leg() if not args.skip_integrator else None
     ens = ensemble_leg() if not args.skip_integrator else None
+    ens_small = small_ensemble_leg() if not args.skip_integrator else None
 
     if rank != 0:
         dist_barrier(world)
@@ -379,6 +380,7 @@ def run_ours(args):
         "device_integrator": integ,
         "reference_gpu_recompiled": ref_gpu,
         "ensemble": ens,
+        "ensemble_small_clusters": ens_small,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
@@ -444,11 +446,14 @@ def run_profile_case(case: str):
 
 def device_integrator_leg(configs=("c1", "c2")):
     """Block-step time of the device-resident integrator (corrector and
-    scheduler on the GPU, 32 block steps per CUDA-graph replay) on the
-    plain-FP64 configurations c1 and c2 of hermite_b200.run_app (eta = 0.01:
-    the mixed path is not used at such small eta, where FP32 force noise
-    collapses the Aarseth steps): wall time per block step, particle steps x
-    N / time, and the energy error."""
+    scheduler on the GPU) on the plain-FP64 configurations c1 and c2 of
+    hermite_b200.run_app (eta = 0.01: the mixed path is not used at such
+    small eta, where FP32 force noise collapses the Aarseth steps): wall time
+    per block step, particle steps x N / time, and the energy error.  c1
+    (N = 1024) runs on both engines: "team" (one thread-block cluster, the
+    whole loop in one kernel; the automatic choice at this N) and "graph"
+    (four kernels per step over the whole GPU, 32 steps per CUDA-graph
+    replay; the automatic choice for c2)."""
     from hermite_b200 import Gravity
     from hermite_b200.ic import plummer, records
     from hermite_b200.run_app import CONFIGS
@@ -459,8 +464,12 @@ def device_integrator_leg(configs=("c1", "c2")):
             cfg["tend"] = 1.0 / 64          # a window: the full run is ~1e7 block steps
         order, n = cfg["order"], cfg["n"]
         eps2 = cfg["eps"] ** 2
-        for prec in ("fp64",):
+        engines = ("team", "graph") if name == "c1" else ("auto",)
+        for eng in engines:
+            prec = "fp64"
             with Gravity(order, n, prec) as g:
+                g.set_engine(eng)
+                used = g.engine()
                 g.set_jp_records(records(plummer(n, 0), order))
                 g.integrator_init(0.0, eps2, cfg["eta"], cfg["eta_s"], 1.0 / cfg["dtmaxinv"])
                 ke0, pe0 = g.energy(eps2)
@@ -470,11 +479,44 @@ def device_integrator_leg(configs=("c1", "c2")):
                 ps, bs, t = g.integrator_stats()
                 ke, pe = g.energy(eps2)
             e0 = ke0 + pe0
-            out[f"{name}_{prec}"] = {
+            key = f"{name}_{prec}" if eng != "graph" else f"{name}_{prec}_graph"
+            out[key] = {
+                "engine": used[0], "team_ctas": used[1],
                 "order": order, "n": n, "tend": cfg["tend"], "block_steps": bs,
                 "particle_steps": ps, "nact_mean": ps / max(bs, 1), "wall_s": wall,
                 "us_per_block": wall / max(bs, 1) * 1e6, "gint_s": ps * n / wall * 1e-9,
                 "de_global": (e0 - (ke + pe)) / e0}
+    return out
+
+
+def small_ensemble_leg(nclusters=256, tend=1.0 / 16):
+    """256 clusters with N log-uniform in [256, 4096] (otherwise as the
+    ensemble leg: power-law masses, eps = 4/N, 6th order FP64, eta = 0.1,
+    dtmax = 1/16), t = 0..tend, on the lockstep engine and on the team
+    engine (every cluster on its own block steps): wall time, Gint/s and the
+    per-cluster block steps summed (equal on both engines)."""
+    from hermite_b200 import Ensemble
+    from hermite_b200.ic import plummer, power_law_masses, records
+    rng = np.random.default_rng(2024)
+    sizes = [int(round(np.exp(rng.uniform(np.log(256), np.log(4096))))) for _ in range(nclusters)]
+    recs = [records(plummer(n, seed=c, masses=power_law_masses(n, np.random.default_rng(c))), 6)
+            for c, n in enumerate(sizes)]
+    out = {"clusters": nclusters, "n_total": int(sum(sizes)), "order": 6, "precision": "fp64",
+           "eta": 0.1, "dtmax": 1.0 / 16, "tend": tend}
+    for eng in ("graph", "team"):
+        with Ensemble(6, sizes, "fp64") as ens:
+            ens.set_engine(eng)
+            for c, n in enumerate(sizes):
+                ens.set_cluster(c, recs[c], (4.0 / n) ** 2)
+            ens.init(0.0, 0.1, 0.02, 1.0 / 16)
+            t0 = time.perf_counter()
+            ens.run(tend, max_block_steps=400_000)
+            wall = time.perf_counter() - t0
+            ps, bs, t, inter = ens.stats()
+        out["lockstep" if eng == "graph" else "team"] = {
+            "wall_s": wall, "gint_s": inter / wall * 1e-9, "particle_steps": ps,
+            "cluster_block_steps": bs}
+    out["team_speedup"] = out["lockstep"]["wall_s"] / out["team"]["wall_s"]
     return out
 
 
@@ -494,6 +536,7 @@ def ensemble_leg(nclusters=256, tend=1.0 / 16, precision="fp64"):
     out = {"clusters": nclusters, "n_total": int(sum(sizes)), "order": 6, "precision": precision,
            "eta": 0.1, "eta_s": 0.02, "dtmax": 1.0 / 16, "tend": tend}
     with Ensemble(6, sizes, precision) as ens:
+        engine = ens.cluster_engine(0)[0]    # clusters above ~11k fit no team: lockstep
         for c, n in enumerate(sizes):
             r = np.random.default_rng(c)
             snap = plummer(n, seed=c, masses=power_law_masses(n, r))
@@ -506,8 +549,8 @@ def ensemble_leg(nclusters=256, tend=1.0 / 16, precision="fp64"):
         ps, bs, t, inter = ens.stats()
         ke1, pe1 = ens.energy()
     de = (ke0 + pe0 - ke1 - pe1) / (ke0 + pe0)
-    out.update({"wall_s": wall, "block_steps": bs, "particle_steps": ps,
-                "us_per_block": wall / max(bs, 1) * 1e6, "gint_s": inter / wall * 1e-9,
+    out.update({"engine": "lockstep" if engine == "graph" else "team", "wall_s": wall,
+                "cluster_block_steps": bs, "particle_steps": ps, "gint_s": inter / wall * 1e-9,
                 "de_global_max_abs": float(np.max(np.abs(de))),
                 "de_global_median_abs": float(np.median(np.abs(de)))})
     return out

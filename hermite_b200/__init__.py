@@ -49,7 +49,8 @@ EXPORTED_SYMBOLS = (
     "hb_integrator_set_engine", "hb_integrator_engine",
     "hb_get_records", "hb_ens_create", "hb_ens_destroy", "hb_ens_last_error",
     "hb_ens_set_cluster", "hb_ens_get_cluster", "hb_ens_cluster_offset", "hb_ens_init",
-    "hb_ens_run", "hb_ens_stats", "hb_ens_energy",
+    "hb_ens_run", "hb_ens_stats", "hb_ens_energy", "hb_ens_set_engine", "hb_ens_cluster_engine",
+    "hb_ens_cluster_stats",
 )
 
 
@@ -130,6 +131,10 @@ def load_library() -> ctypes.CDLL:
         "hb_ens_stats": (I, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                              dp, dp]),
         "hb_ens_energy": (I, [P, dp, dp]),
+        "hb_ens_set_engine": (I, [P, I, I]),
+        "hb_ens_cluster_engine": (I, [P, I, ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "hb_ens_cluster_stats": (I, [P, I, ctypes.POINTER(ctypes.c_longlong),
+                                     ctypes.POINTER(ctypes.c_longlong), dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -304,8 +309,8 @@ class Gravity:
 
 
 class Ensemble:
-    """Independent clusters integrated together on the device (batched
-    block steps; each particle interacts only with its own cluster)."""
+    """Independent clusters integrated together on the device; each particle
+    interacts only with its own cluster."""
 
     def __init__(self, order: int, sizes, precision="mixed"):
         self._lib = load_library()
@@ -363,7 +368,30 @@ class Ensemble:
     def run(self, tend: float, max_block_steps: int = 0):
         self._check(self._lib.hb_ens_run(self._h, float(tend), int(max_block_steps)), "run")
 
+    def set_engine(self, engine: str = "auto", team_ctas: int = 0):
+        """"auto", "graph" (lockstep over the union of clusters) or "team"
+        (each cluster on its own block steps, one thread-block cluster each)."""
+        self._check(self._lib.hb_ens_set_engine(self._h, ENGINES[engine], int(team_ctas)),
+                    "set_engine")
+
+    def cluster_engine(self, c: int):
+        """("team", CTAs) or ("graph", 0): how run() integrates cluster c."""
+        e, k = ctypes.c_int(), ctypes.c_int()
+        self._check(self._lib.hb_ens_cluster_engine(self._h, int(c), ctypes.byref(e),
+                                                    ctypes.byref(k)), "cluster_engine")
+        return {v: n for n, v in ENGINES.items()}[e.value], k.value
+
+    def cluster_stats(self, c: int):
+        """(particle steps, block steps, time) of cluster c."""
+        ps, bs, t = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
+        self._check(self._lib.hb_ens_cluster_stats(self._h, int(c), ctypes.byref(ps),
+                                                   ctypes.byref(bs), ctypes.byref(t)),
+                    "cluster_stats")
+        return ps.value, bs.value, t.value
+
     def stats(self):
+        """Sums over clusters: (particle steps, block steps, earliest time,
+        interactions)."""
         ps, bs = ctypes.c_longlong(), ctypes.c_longlong()
         t, inter = ctypes.c_double(), ctypes.c_double()
         self._check(self._lib.hb_ens_stats(self._h, ctypes.byref(ps), ctypes.byref(bs),

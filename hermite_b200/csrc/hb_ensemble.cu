@@ -42,6 +42,13 @@ struct Cluster {
     double eps2;
 };
 
+// Clusters integrated by team kernels of one size: systems [first,
+// first + count) of the team system table.
+struct TeamGroup {
+    int ctas, first, count;
+    TeamConfig cfg;
+};
+
 // Programmatic dependent launch (see hb_integrator.cu): schedule the next
 // kernel now, wait for the previous kernel's results.
 __device__ __forceinline__ void pdl_enter()
@@ -71,15 +78,28 @@ struct EnsSched {
 struct EnsLaunch {
     double *jp, *dt, *force, *partial;
     int *ilist, *ccnt, *tile_base;     // tile_base[nclusters + 1]
+    int *item_base, *pitem_base;       // per-cluster force items / partial slots, prefix sums
     unsigned *counter;
     const Cluster *cl;
     const int *slot_cluster;           // per 128-slot block
+    TeamState *cst;                    // per-cluster state and counters
     EnsSched *s;
     int *err;
     int nslot, nclusters, nsm;
     size_t partial_cap;
     int target_items, items_grid, smem;
 };
+
+// j-slices of one i-tile of a cluster with cnt active slots in npad slots:
+// a function of the cluster alone (up to 16 slices when it has few active
+// tiles, none thinner than 4 chunks), so that a cluster's forces -- and its
+// block steps -- do not depend on the other clusters of the ensemble.
+__device__ __forceinline__ int ens_split(int cnt, int npad)
+{
+    const int tiles = (cnt + 31) / 32;
+    if (tiles == 0) return 0;
+    return max(1, min(16 / tiles, npad / 128));
+}
 
 // 1. next block time; reset the per-cluster counters
 template <int ORDER>
@@ -137,32 +157,60 @@ __global__ void ens_compact_kernel(EnsLaunch L)
 __global__ void ens_tiles_kernel(EnsLaunch L)
 {
     pdl_enter();
-    __shared__ int part[1024];
+    __shared__ int part[1024], ipart[1024], ppart[1024];
     const int per = (L.nclusters + blockDim.x - 1) / blockDim.x;
     const int c0 = threadIdx.x * per, c1 = min(L.nclusters, c0 + per);
-    int tiles = 0, act = 0;
+    int tiles = 0, act = 0, items = 0, pitems = 0;
+    const double tnext = L.s->tnext;
     for (int c = c0; c < c1; ++c) {
-        tiles += (L.ccnt[c] + 31) / 32;
-        act += L.ccnt[c];
+        const int k = L.ccnt[c];
+        const int tl = (k + 31) / 32, sc = ens_split(k, L.cl[c].npad);
+        tiles += tl;
+        items += tl * sc;
+        pitems += sc > 1 ? tl * sc : 0;
+        act += k;
+        if (k > 0) {   // this cluster takes a block step at tnext
+            TeamState &t = L.cst[c];
+            t.tsys = tnext;
+            t.particle_steps += k;
+            t.block_steps += 1;
+            t.interactions += (double)k * L.cl[c].n;
+        }
     }
     part[threadIdx.x] = tiles;
+    ipart[threadIdx.x] = items;
+    ppart[threadIdx.x] = pitems;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int run = 0;
+        int run = 0, irun = 0, prun = 0;
         for (int t = 0; t < (int)blockDim.x; ++t) {
-            const int v = part[t];
+            const int v = part[t], iv = ipart[t], pv = ppart[t];
             part[t] = run;
+            ipart[t] = irun;
+            ppart[t] = prun;
             run += v;
+            irun += iv;
+            prun += pv;
         }
         L.s->total_tiles = run;
     }
     __syncthreads();
-    int run = part[threadIdx.x];
+    int run = part[threadIdx.x], irun = ipart[threadIdx.x], prun = ppart[threadIdx.x];
     for (int c = c0; c < c1; ++c) {
+        const int k = L.ccnt[c];
+        const int tl = (k + 31) / 32, sc = ens_split(k, L.cl[c].npad);
         L.tile_base[c] = run;
-        run += (L.ccnt[c] + 31) / 32;
+        L.item_base[c] = irun;
+        L.pitem_base[c] = prun;
+        run += tl;
+        irun += tl * sc;
+        prun += sc > 1 ? tl * sc : 0;
     }
-    if (threadIdx.x == blockDim.x - 1) L.tile_base[L.nclusters] = run;
+    if (threadIdx.x == blockDim.x - 1) {
+        L.tile_base[L.nclusters] = run;
+        L.item_base[L.nclusters] = irun;
+        L.pitem_base[L.nclusters] = prun;
+    }
     // totals for the statistics
     __shared__ int sact[1024];
     sact[threadIdx.x] = act;
@@ -178,6 +226,51 @@ __global__ void ens_tiles_kernel(EnsLaunch L)
             L.s->block_steps += 1;
             L.s->interactions += inter;
         }
+    }
+}
+
+// Sums of the per-cluster counters (fixed order), minimum time, any error.
+struct EnsTotals {
+    double tmin, interactions;
+    long long particle_steps, block_steps;
+    int error, pad;
+};
+
+__global__ void ens_totals_kernel(const TeamState *st, const int *idx, int n, EnsTotals *out)
+{
+    __shared__ double s_t[256], s_i[256];
+    __shared__ long long s_p[256], s_b[256];
+    __shared__ int s_e[256];
+    double t = __longlong_as_double(0x7ff0000000000000ll), in = 0.0;
+    long long ps = 0, bs = 0;
+    int er = 0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const TeamState &x = st[idx ? idx[k] : k];
+        t = fmin(t, x.tsys);
+        in += x.interactions;
+        ps += x.particle_steps;
+        bs += x.block_steps;
+        er |= x.error;
+    }
+    s_t[threadIdx.x] = t;
+    s_i[threadIdx.x] = in;
+    s_p[threadIdx.x] = ps;
+    s_b[threadIdx.x] = bs;
+    s_e[threadIdx.x] = er;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < (int)blockDim.x; ++k) {
+            t = fmin(t, s_t[k]);
+            in += s_i[k];
+            ps += s_p[k];
+            bs += s_b[k];
+            er |= s_e[k];
+        }
+        out->tmin = t;
+        out->interactions = in;
+        out->particle_steps = ps;
+        out->block_steps = bs;
+        out->error = er;
     }
 }
 
@@ -197,15 +290,10 @@ ens_force_kernel(EnsLaunch L)
     __shared__ int s_item;
     __shared__ unsigned s_last;
 
-    const int T = L.s->total_tiles;
-    if (T == 0) return;
+    const int items = L.item_base[L.nclusters];
+    if (items == 0) return;
     const double tsys = L.s->tnext;
     const int tid = threadIdx.x, lane = tid & 31, jg = tid >> 5;
-    int S = (L.target_items + T - 1) / T;
-    S = max(1, min(S, 16));
-    while (S > 1 && (size_t)S * T * TI * F > L.partial_cap) --S;
-    const int items = T * S;
-    const size_t tspan = (size_t)T * TI;
 
     if (tid == 0) {
         mbar_init(&bar[0], 1);
@@ -219,17 +307,20 @@ ens_force_kernel(EnsLaunch L)
         __syncthreads();
         const int item = s_item;
         if (item >= items) break;
-        const int tile = item / S, sl = item % S;
-        // the tile's cluster: last c with tile_base[c] <= tile
+        // the item's cluster: last c with item_base[c] <= item
         int lo = 0, hi = L.nclusters - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (L.tile_base[mid] <= tile) lo = mid; else hi = mid - 1;
+            if (L.item_base[mid] <= item) lo = mid; else hi = mid - 1;
         }
         const int c = lo;
         const Cluster cl = L.cl[c];
         const int cnt = L.ccnt[c];
-        const int k0 = (tile - L.tile_base[c]) * TI;
+        const int S = ens_split(cnt, cl.npad);
+        const int li = item - L.item_base[c], tl = li / S, sl = li - tl * S;
+        const int tile = L.tile_base[c] + tl;
+        const size_t pslot = (size_t)L.pitem_base[c] + (size_t)tl * S;   // partials of this tile
+        const int k0 = tl * TI;
         const double eps2 = cl.eps2;
 
         double *raw = reinterpret_cast<double *>(smem);
@@ -314,7 +405,7 @@ ens_force_kernel(EnsLaunch L)
             } else {
 #pragma unroll
                 for (int q = 0; q < F; ++q)
-                    L.partial[((size_t)sl * tspan + (size_t)tile * TI + lane) * F + q] = f[0][q];
+                    L.partial[((pslot + sl) * TI + lane) * F + q] = f[0][q];
             }
         }
         if (S > 1) {
@@ -325,10 +416,10 @@ ens_force_kernel(EnsLaunch L)
             if (s_last) {
                 __threadfence();
                 const int V = min(TI, cnt - k0) * F;
-                const double *pbase = L.partial + (size_t)tile * TI * F;
+                const double *pbase = L.partial + pslot * TI * F;
                 for (int e = tid; e < V; e += NW * 32) {
                     double sum = 0.0;
-                    for (int s2 = 0; s2 < S; ++s2) sum += __ldcg(pbase + (size_t)s2 * tspan * F + e);
+                    for (int s2 = 0; s2 < S; ++s2) sum += __ldcg(pbase + (size_t)s2 * TI * F + e);
                     L.force[((size_t)cl.off + k0) * F + e] = sum;
                 }
                 if (tid == 0) L.counter[tile] = 0u;
@@ -517,6 +608,7 @@ struct hb_ens {
     double *d_jp = nullptr, *d_dt = nullptr, *d_force = nullptr, *d_partial = nullptr,
            *d_pot = nullptr, *h_eout = nullptr, *d_eout = nullptr;
     int *d_ilist = nullptr, *d_ccnt = nullptr, *d_tile_base = nullptr, *d_slot_cluster = nullptr;
+    int *d_item_base = nullptr, *d_pitem_base = nullptr;
     unsigned *d_counter = nullptr;
     Cluster *d_cl = nullptr;
     EnsSched *h_s = nullptr, *d_s = nullptr;       // host copy (set-up) / device
@@ -528,6 +620,16 @@ struct hb_ens {
     bool ready = false;
     std::string err;
     EnsLaunch L;
+    // per-cluster state (both engines) and the team engine
+    TeamState *d_cstate = nullptr;
+    EnsTotals *h_tot = nullptr, *d_tot = nullptr;   // mapped
+    TeamSys *d_tsys = nullptr;                      // team systems, grouped by team size
+    int *d_tidx = nullptr;                          // their cluster indices
+    int *d_team_next = nullptr;
+    int engine = HB_ENGINE_AUTO, team_ctas = 0;
+    std::vector<TeamGroup> groups;                  // built for (engine, team_ctas)
+    std::vector<int> cluster_ctas;                  // per cluster: team size, 0 = lockstep engine
+    bool groups_ready = false;
 };
 
 namespace {
@@ -543,6 +645,149 @@ int ens_fail(hb_ens *e, int status, const char *msg, cudaError_t ce = cudaSucces
         }
     }
     return status;
+}
+
+// Team size for a cluster of n particles: at least n / kEnsTeamSlots CTAs
+// (a power of two), more if its slots do not fit the CTAs' shared memory.
+constexpr int kEnsTeamSlots = 512;
+constexpr long long kEnsTeamStepsPerLaunch = 1LL << 14;
+
+int build_groups(hb_ens *e)
+{
+    if (e->groups_ready) return HB_OK;
+    e->groups.clear();
+    e->cluster_ctas.assign(e->nclusters, 0);
+    if (e->engine == HB_ENGINE_GRAPH) {
+        e->groups_ready = true;
+        return HB_OK;
+    }
+    if (e->precision != HB_FP64) {
+        if (e->engine == HB_ENGINE_TEAM)
+            return ens_fail(e, HB_ERR_INVALID, "the team engine integrates in FP64 only");
+        e->groups_ready = true;
+        return HB_OK;
+    }
+    TeamConfig cfgs[17] = {};
+    bool tried[17] = {};
+    auto cfg_for = [&](int C) -> const TeamConfig * {
+        if (!tried[C]) {
+            tried[C] = true;
+            if (team_setup(e->order, C, &cfgs[C]) != cudaSuccess || cfgs[C].max_teams < 1) {
+                cudaGetLastError();
+                cfgs[C].ctas = 0;
+            }
+        }
+        return cfgs[C].ctas ? &cfgs[C] : nullptr;
+    };
+    std::vector<std::vector<int>> by(17);
+    for (int c = 0; c < e->nclusters; ++c) {
+        const int n = e->cl[c].n, nch = (n + 31) / 32;
+        int C = e->team_ctas;
+        if (C == 0) {
+            C = 1;
+            while (C < 16 && (long long)C * kEnsTeamSlots < n) C <<= 1;
+        }
+        for (;;) {
+            const TeamConfig *cf = cfg_for(C);
+            if (cf && (long long)((nch + C - 1) / C) * 32 <= cf->jl_cap) break;
+            if (e->team_ctas > 0 || C >= 16) {
+                C = 0;
+                break;
+            }
+            C <<= 1;
+        }
+        if (C == 0) continue;   // the lockstep engine takes it
+        by[C].push_back(c);
+        e->cluster_ctas[c] = C;
+    }
+    if (e->engine == HB_ENGINE_AUTO) {
+        // all or nothing: a team phase followed by a lockstep phase for the
+        // rest would leave most of the GPU idle in the tail of each
+        bool all = true;
+        for (int C : e->cluster_ctas) all &= C > 0;
+        if (!all) {
+            e->cluster_ctas.assign(e->nclusters, 0);
+            e->groups_ready = true;
+            return HB_OK;
+        }
+    }
+    std::vector<TeamSys> ts;
+    std::vector<int> idx;
+    for (int C = 1; C <= 16; ++C) {
+        if (by[C].empty()) continue;
+        std::vector<int> &v = by[C];
+        // largest systems first: the queue's tail is short
+        std::stable_sort(v.begin(), v.end(), [&](int a, int b) { return e->cl[a].n > e->cl[b].n; });
+        TeamGroup g;
+        g.ctas = C;
+        g.first = (int)ts.size();
+        g.count = (int)v.size();
+        g.cfg = cfgs[C];
+        for (int c : v) {
+            TeamSys t;
+            t.off = e->cl[c].off;
+            t.n = e->cl[c].n;
+            t.id = c;
+            t.eps2 = e->cl[c].eps2;
+            ts.push_back(t);
+            idx.push_back(c);
+        }
+        e->groups.push_back(g);
+    }
+    if (!ts.empty()) {
+        cudaError_t ce = cudaMemcpy(e->d_tsys, ts.data(), ts.size() * sizeof(TeamSys), cudaMemcpyHostToDevice);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpy(e->d_tidx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice);
+        if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "team system table", ce);
+    }
+    e->groups_ready = true;
+    return HB_OK;
+}
+
+// Sums of the per-cluster counters over `count` clusters (all when idx is null).
+int totals(hb_ens *e, const int *idx, int count)
+{
+    ens_totals_kernel<<<1, 256, 0, e->stream>>>(e->d_cstate, idx, count, e->d_tot);
+    cudaError_t ce = cudaGetLastError();
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    return ce == cudaSuccess ? HB_OK : ens_fail(e, HB_ERR_CUDA, "cluster totals", ce);
+}
+
+// Every team-engine cluster integrated to tend, one group of team size at a time.
+int run_teams(hb_ens *e, double tend, long long max_block_steps)
+{
+    for (const TeamGroup &g : e->groups) {
+        TeamLaunch L;
+        L.jp = e->d_jp;
+        L.dt = e->d_dt;
+        L.sys = e->d_tsys + g.first;
+        L.st = e->d_cstate;
+        L.next_sys = e->d_team_next;
+        L.nsys = g.count;
+        L.ctas = g.ctas;
+        L.jl_cap = g.cfg.jl_cap;
+        L.smem = g.cfg.smem;
+        L.tend = tend;
+        L.etapow = e->h_s->etapow;
+        L.dtmax = e->h_s->dtmax;
+        L.max_steps = max_block_steps > 0 ? max_block_steps : kEnsTeamStepsPerLaunch;
+        const int teams = std::min(g.cfg.max_teams, g.count);
+        double last = -1.0;
+        for (;;) {
+            cudaError_t ce = cudaMemsetAsync(e->d_team_next, 0, sizeof(int), e->stream);
+            if (ce == cudaSuccess) ce = team_launch(e->order, L, teams, e->stream);
+            if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "team launch", ce);
+            const int s = totals(e, e->d_tidx + g.first, g.count);
+            if (s != HB_OK) return s;
+            const volatile EnsTotals *t = e->h_tot;
+            if (t->error) return ens_fail(e, HB_ERR_STATE, "a timestep underflowed (< 2^-48)");
+            if (t->tmin >= tend) break;
+            if (max_block_steps > 0) return ens_fail(e, HB_ERR_STATE, "block-step limit reached");
+            if (t->tmin == last) return ens_fail(e, HB_ERR_STATE, "ensemble integration stalled");
+            last = t->tmin;
+        }
+    }
+    return HB_OK;
 }
 
 cudaError_t dispatch_step(hb_ens *e)
@@ -573,6 +818,8 @@ int hb_ens_destroy(hb_ens *e)
     cudaFree(e->d_ilist);
     cudaFree(e->d_ccnt);
     cudaFree(e->d_tile_base);
+    cudaFree(e->d_item_base);
+    cudaFree(e->d_pitem_base);
     cudaFree(e->d_slot_cluster);
     cudaFree(e->d_counter);
     cudaFree(e->d_cl);
@@ -581,6 +828,11 @@ int hb_ens_destroy(hb_ens *e)
     cudaFreeHost(e->h_st);
     cudaFreeHost(e->h_eout);
     cudaFreeHost(e->h_err);
+    cudaFree(e->d_cstate);
+    cudaFreeHost(e->h_tot);
+    cudaFree(e->d_tsys);
+    cudaFree(e->d_tidx);
+    cudaFree(e->d_team_next);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
     return HB_OK;
@@ -627,7 +879,8 @@ int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_
         off += k.npad;
     }
     const size_t ns = e->nslot;
-    e->partial_cap = (size_t)2 * e->nsm * 8 * 256 * e->F;
+    // a cluster with j-split tiles has at most 16 (tile, slice) items
+    e->partial_cap = (size_t)16 * nclusters * 32 * e->F;
     bool ok = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc((void **)&e->d_jp, ns * e->R * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_dt, ns * sizeof(double)) == cudaSuccess &&
@@ -637,6 +890,8 @@ int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_
               cudaMalloc((void **)&e->d_ilist, ns * sizeof(int)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_ccnt, nclusters * sizeof(int)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_tile_base, (nclusters + 1) * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_item_base, (nclusters + 1) * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_pitem_base, (nclusters + 1) * sizeof(int)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_slot_cluster, slot_cluster.size() * sizeof(int)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_counter, (ns / 32 + nclusters + 1) * sizeof(unsigned)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_cl, nclusters * sizeof(Cluster)) == cudaSuccess &&
@@ -646,7 +901,13 @@ int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_
               cudaHostAlloc((void **)&e->h_eout, 2 * nclusters * sizeof(double), cudaHostAllocMapped) == cudaSuccess &&
               cudaHostGetDevicePointer((void **)&e->d_eout, e->h_eout, 0) == cudaSuccess &&
               cudaHostAlloc((void **)&e->h_err, sizeof(int), cudaHostAllocMapped) == cudaSuccess &&
-              cudaHostGetDevicePointer((void **)&e->d_err, e->h_err, 0) == cudaSuccess;
+              cudaHostGetDevicePointer((void **)&e->d_err, e->h_err, 0) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_cstate, nclusters * sizeof(TeamState)) == cudaSuccess &&
+              cudaHostAlloc((void **)&e->h_tot, sizeof(EnsTotals), cudaHostAllocMapped) == cudaSuccess &&
+              cudaHostGetDevicePointer((void **)&e->d_tot, e->h_tot, 0) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_tsys, nclusters * sizeof(TeamSys)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_tidx, nclusters * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_team_next, sizeof(int)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         hb_ens_destroy(e);
@@ -680,9 +941,12 @@ int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_
     L.ilist = e->d_ilist;
     L.ccnt = e->d_ccnt;
     L.tile_base = e->d_tile_base;
+    L.item_base = e->d_item_base;
+    L.pitem_base = e->d_pitem_base;
     L.counter = e->d_counter;
     L.cl = e->d_cl;
     L.slot_cluster = e->d_slot_cluster;
+    L.cst = e->d_cstate;
     L.s = e->d_s;
     L.err = e->d_err;
     L.nslot = e->nslot;
@@ -721,6 +985,7 @@ int hb_ens_set_cluster(hb_ens *e, int c, const double *records, double eps2)
 {
     if (!e || c < 0 || c >= e->nclusters || !records || !(eps2 >= 0.0)) return HB_ERR_INVALID;
     e->cl[c].eps2 = eps2;
+    e->groups_ready = false;
     cudaError_t ce = cudaMemcpyAsync(e->d_jp + (size_t)e->cl[c].off * e->R, records,
                                      sizeof(double) * (size_t)e->cl[c].n * e->R,
                                      cudaMemcpyHostToDevice, e->stream);
@@ -802,6 +1067,14 @@ int hb_ens_init(hb_ens *e, double tsys, double eta, double eta_s, double dtmax)
     if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "scheduler upload", ce);
     std::memset(e->h_st, 0, sizeof(EnsStatus));
     e->h_st->tsys = tsys;
+    std::vector<TeamState> cs(e->nclusters);
+    for (TeamState &t : cs) {
+        std::memset(&t, 0, sizeof t);
+        t.tsys = tsys;
+    }
+    ce = cudaMemcpy(e->d_cstate, cs.data(), cs.size() * sizeof(TeamState), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "cluster state", ce);
+    e->groups_ready = false;
     ce = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
     if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "capture", ce);
     cudaError_t le = cudaSuccess;
@@ -826,6 +1099,18 @@ int hb_ens_run(hb_ens *e, double tend, long long max_block_steps)
     if (!e->ready) return ens_fail(e, HB_ERR_STATE, "hb_ens_run before hb_ens_init");
     cudaError_t ce = cudaStreamSynchronize(e->stream);
     if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "sync", ce);
+    int s0 = build_groups(e);
+    if (s0 == HB_OK) s0 = totals(e, nullptr, e->nclusters);
+    if (s0 != HB_OK) return s0;
+    if (!(tend >= e->h_tot->tmin)) return ens_fail(e, HB_ERR_INVALID, "tend is before tsys");
+    s0 = run_teams(e, tend, max_block_steps);
+    if (s0 != HB_OK) return s0;
+    bool lockstep = false;
+    for (int c : e->cluster_ctas) lockstep |= c == 0;
+    if (!lockstep) return HB_OK;
+
+    // the lockstep engine: the other clusters (those already at tend have
+    // no active particles until tend)
     volatile EnsStatus *st = e->h_st;
     if (!(tend >= st->tsys)) return ens_fail(e, HB_ERR_INVALID, "tend is before tsys");
     ce = cudaMemcpy(&e->d_s->tend, &tend, sizeof(double), cudaMemcpyHostToDevice);
@@ -849,15 +1134,52 @@ int hb_ens_run(hb_ens *e, double tend, long long max_block_steps)
     return HB_OK;
 }
 
-int hb_ens_stats(const hb_ens *e, long long *particle_steps, long long *block_steps, double *tsys,
+int hb_ens_stats(hb_ens *e, long long *particle_steps, long long *block_steps, double *tsys,
                  double *interactions)
 {
     if (!e) return HB_ERR_INVALID;
-    const volatile EnsStatus *s = e->h_st;
-    if (particle_steps) *particle_steps = s->particle_steps;
-    if (block_steps) *block_steps = s->block_steps;
-    if (tsys) *tsys = s->tsys;
-    if (interactions) *interactions = s->interactions;
+    const int s = totals(e, nullptr, e->nclusters);
+    if (s != HB_OK) return s;
+    const volatile EnsTotals *t = e->h_tot;
+    if (particle_steps) *particle_steps = t->particle_steps;
+    if (block_steps) *block_steps = t->block_steps;
+    if (tsys) *tsys = t->tmin;
+    if (interactions) *interactions = t->interactions;
+    return HB_OK;
+}
+
+int hb_ens_cluster_stats(hb_ens *e, int c, long long *particle_steps, long long *block_steps,
+                         double *tsys)
+{
+    if (!e || c < 0 || c >= e->nclusters) return HB_ERR_INVALID;
+    TeamState t;
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpy(&t, e->d_cstate + c, sizeof t, cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "cluster stats", ce);
+    if (particle_steps) *particle_steps = t.particle_steps;
+    if (block_steps) *block_steps = t.block_steps;
+    if (tsys) *tsys = t.tsys;
+    return HB_OK;
+}
+
+int hb_ens_set_engine(hb_ens *e, int engine, int team_ctas)
+{
+    if (!e || engine < HB_ENGINE_AUTO || engine > HB_ENGINE_TEAM || team_ctas < 0 || team_ctas > 16)
+        return HB_ERR_INVALID;
+    e->engine = engine;
+    e->team_ctas = team_ctas;
+    e->groups_ready = false;
+    return HB_OK;
+}
+
+int hb_ens_cluster_engine(hb_ens *e, int c, int *engine, int *team_ctas)
+{
+    if (!e || c < 0 || c >= e->nclusters) return HB_ERR_INVALID;
+    const int s = build_groups(e);
+    if (s != HB_OK) return s;
+    const int C = e->cluster_ctas[c];
+    if (engine) *engine = C ? HB_ENGINE_TEAM : HB_ENGINE_GRAPH;
+    if (team_ctas) *team_ctas = C;
     return HB_OK;
 }
 

@@ -77,7 +77,8 @@ constexpr int kTeamIMax = 256;              // active slots per force round
 constexpr int kTeamMaxSlotsPerCta = 2048;
 struct TeamSys {
     long long off;     // first slot of the system in the record / dt arrays
-    int n, pad;
+    int n;
+    int id;            // index of the system's TeamState
     double eps2;
 };
 struct TeamState {     // per system, persistent across launches
@@ -95,7 +96,7 @@ struct TeamConfig {
 struct TeamLaunch {
     double *jp, *dt;
     const TeamSys *sys;
-    TeamState *st;
+    TeamState *st;     // indexed by TeamSys::id
     int *next_sys;     // work counter, zero at launch
     int nsys;
     int ctas, jl_cap, smem;

@@ -184,8 +184,8 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
             }
         }
         if (tid == 0) misc[1] = 0;
-        double tsys = L.st[sidx].tsys;
-        const bool dead = L.st[sidx].error != 0;   // a system that failed stays stopped
+        double tsys = L.st[S.id].tsys;
+        const bool dead = L.st[S.id].error != 0;   // a system that failed stays stopped
         long long steps = 0, psteps = 0;
         double inter = 0.0;
         int err = 0;
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
         for (int q = tid; q < JL; q += T)
             if (lo + q < n) dtg[lo + q] = dts[q];
         if (rank == 0 && tid == 0) {
-            TeamState &st = L.st[sidx];
+            TeamState &st = L.st[S.id];
             st.tsys = tsys;
             st.particle_steps += psteps;
             st.block_steps += steps;

@@ -208,12 +208,34 @@ int hb_ens_get_cluster(hb_ens *ens, int c, double *records, double *dt_out);
 int hb_ens_cluster_offset(const hb_ens *ens, int c);
 /* init_step for every cluster (bootstrap forces, initial dt). */
 int hb_ens_init(hb_ens *ens, double tsys, double eta, double eta_s, double dtmax);
-/* Integrate all clusters until tend (max_block_steps as hb_integrator_run). */
+/* Engines for hb_ens_run (HB_ENGINE_* as for hb_integrator_set_engine):
+ *  HB_ENGINE_GRAPH  lockstep: one global block-step loop over the union of
+ *                   all clusters, five kernels per step from a CUDA graph;
+ *  HB_ENGINE_TEAM   every cluster that fits a team of up to 16 CTAs on its
+ *                   own block-time sequence: one thread-block cluster of
+ *                   team_ctas CTAs (0: chosen per cluster from its size)
+ *                   integrates one cluster at a time from a device queue,
+ *                   largest first (FP64); the clusters that do not fit
+ *                   follow on the lockstep engine;
+ *  HB_ENGINE_AUTO   the team engine when every cluster fits a team (FP64),
+ *                   else the lockstep engine for all (the default).
+ * Per cluster both engines integrate the same algorithm; a cluster's
+ * result does not depend on the other clusters. */
+int hb_ens_set_engine(hb_ens *ens, int engine, int team_ctas);
+/* The engine (HB_ENGINE_TEAM / HB_ENGINE_GRAPH) and team size that
+ * hb_ens_run uses for cluster c. */
+int hb_ens_cluster_engine(hb_ens *ens, int c, int *engine, int *team_ctas);
+/* Integrate all clusters until tend (max_block_steps as hb_integrator_run,
+ * counted per cluster for the team engine). */
 int hb_ens_run(hb_ens *ens, double tend, long long max_block_steps);
-/* Sums over block steps since init: particle steps, block steps, the
- * current time, and interactions (sum of nact_c * N_c). */
-int hb_ens_stats(const hb_ens *ens, long long *particle_steps, long long *block_steps,
+/* Sums over clusters since init: particle steps, block steps (each
+ * cluster's own), the earliest cluster time, and interactions (sum over
+ * block steps of nact_c * N_c). */
+int hb_ens_stats(hb_ens *ens, long long *particle_steps, long long *block_steps,
                  double *tsys, double *interactions);
+/* One cluster's particle steps, block steps and time. */
+int hb_ens_cluster_stats(hb_ens *ens, int c, long long *particle_steps, long long *block_steps,
+                         double *tsys);
 /* Per-cluster kinetic and potential energy (arrays of nclusters). */
 int hb_ens_energy(hb_ens *ens, double *kinetic, double *potential);
 
