@@ -761,9 +761,8 @@ int run_team(hb_ctx *ctx, const TeamConfig &cfg, double tend, long long max_bloc
     L.st = ctx->d_team_state;
     L.next_sys = ctx->d_team_next;
     L.nsys = 1;
-    L.ctas = cfg.ctas;
-    L.jl_cap = cfg.jl_cap;
-    L.smem = cfg.smem;
+    if (team_shape(ctx->order, cfg, ctx->nbody, &L) != 0)
+        return fail(ctx, HB_ERR_TOO_LARGE, "the system does not fit a team of %d CTAs", cfg.ctas);
     L.tend = tend;
     L.etapow = ctx->h_sched->etapow;
     L.dtmax = ctx->h_sched->dtmax;

@@ -45,7 +45,7 @@ struct Cluster {
 // Clusters integrated by team kernels of one size: systems [first,
 // first + count) of the team system table.
 struct TeamGroup {
-    int ctas, first, count;
+    int ctas, first, count, nmax;
     TeamConfig cfg;
 };
 
@@ -722,6 +722,7 @@ int build_groups(hb_ens *e)
         g.ctas = C;
         g.first = (int)ts.size();
         g.count = (int)v.size();
+        g.nmax = e->cl[v.front()].n;
         g.cfg = cfgs[C];
         for (int c : v) {
             TeamSys t;
@@ -764,9 +765,8 @@ int run_teams(hb_ens *e, double tend, long long max_block_steps)
         L.st = e->d_cstate;
         L.next_sys = e->d_team_next;
         L.nsys = g.count;
-        L.ctas = g.ctas;
-        L.jl_cap = g.cfg.jl_cap;
-        L.smem = g.cfg.smem;
+        if (team_shape(e->order, g.cfg, g.nmax, &L) != 0)
+            return ens_fail(e, HB_ERR_TOO_LARGE, "a cluster does not fit its team");
         L.tend = tend;
         L.etapow = e->h_s->etapow;
         L.dtmax = e->h_s->dtmax;

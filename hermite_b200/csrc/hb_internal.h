@@ -73,7 +73,7 @@ cudaError_t integrator_step_launch(int order, const IntegratorLaunch &L, cudaStr
 
 // Team engine (hb_team.cu): one thread-block cluster of `ctas` CTAs runs the
 // whole block-step loop of one system at a time inside one kernel.
-constexpr int kTeamIMax = 256;              // active slots per force round
+constexpr int kTeamIMax = 256;              // smallest round of i-states
 constexpr int kTeamMaxSlotsPerCta = 2048;
 struct TeamSys {
     long long off;     // first slot of the system in the record / dt arrays
@@ -89,8 +89,8 @@ struct TeamState {     // per system, persistent across launches
 };
 struct TeamConfig {
     int ctas;          // CTAs per team (cluster size)
-    int jl_cap;        // slots per CTA that fit in shared memory
-    int smem;          // dynamic shared memory per CTA
+    int jl_cap;        // slots per CTA that fit in shared memory (rounds of kTeamIMax)
+    int smem;          // dynamic shared memory available per CTA
     int max_teams;     // co-resident teams on this device
 };
 struct TeamLaunch {
@@ -99,11 +99,14 @@ struct TeamLaunch {
     TeamState *st;     // indexed by TeamSys::id
     int *next_sys;     // work counter, zero at launch
     int nsys;
-    int ctas, jl_cap, smem;
+    int ctas, jl_cap, im, smem;   // from team_shape
     double tend, etapow, dtmax;
     long long max_steps;   // per system and launch
 };
 cudaError_t team_setup(int order, int ctas, TeamConfig *cfg);
+// Fills L's ctas, jl_cap, im and smem for systems of up to nmax particles;
+// -1 when they do not fit a team of cfg.ctas CTAs.
+int team_shape(int order, const TeamConfig &cfg, int nmax, TeamLaunch *L);
 cudaError_t team_launch(int order, const TeamLaunch &L, int teams, cudaStream_t s);
 cudaError_t team_sched_sync(Sched *s, TeamState *st, bool to_team, cudaStream_t stream);
 

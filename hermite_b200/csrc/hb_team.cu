@@ -20,7 +20,8 @@
 //      each owner adds the C partials of its active slots in rank order and
 //      runs the corrector (Particle::correct + the quantised Aarseth step)
 //
-// More than kTeamIMax active slots are processed in rounds of kTeamIMax.
+// Steps with more active slots than the push regions hold are processed in
+// rounds pulled from the owners.
 // Teams take systems from a device counter, so one launch integrates a whole
 // ensemble with every system on its own block-time sequence (no lockstep),
 // or a single system.  The per-system state is the same record array and dt
@@ -53,17 +54,17 @@ struct TeamXch {
     int err;      // a corrector of the sender produced a timestep underflow
 };
 
-// Shared-memory carve-up for a given slots-per-CTA capacity.
+// Shared-memory carve-up for jl own slots per CTA and im i-states per round.
 template <int ORDER>
 struct TeamSmem {
     static constexpr int R = Rec<ORDER>::words, P = Pred64<ORDER>::ncomp, F = Frc<ORDER>::words;
-    static constexpr int IM = kTeamIMax;
-    // fixed: ibuf [IM][P], part [IM][F], xa [16] (doubles); gq, gc [IM], koff [48], misc [4] (ints)
-    static constexpr size_t fixed = (size_t)IM * (P + F) * 8 + 16 * sizeof(TeamXch) +
-                                    (size_t)(2 * IM + 48 + 4) * 4 + 64;
+    // per i-state: ibuf [P], part [F] (doubles); gq, gc (ints)
+    static constexpr size_t per_i = (size_t)(P + F) * 8 + 2 * 4;
     // per slot: record, predicted state, tlast + dt, dt (doubles); candidate (int)
     static constexpr size_t per_slot = (size_t)(R + P + 2) * 8 + 4;
-    static size_t bytes(int jl_cap) { return fixed + per_slot * (size_t)jl_cap; }
+    // xa [16], koff [48], misc [4], alignment
+    static constexpr size_t fixed = 16 * sizeof(TeamXch) + (48 + 4) * 4 + 64;
+    static size_t bytes(int jl, int im) { return fixed + per_i * (size_t)im + per_slot * (size_t)jl; }
 };
 
 __device__ __forceinline__ double warp_min(double v)
@@ -93,7 +94,7 @@ __device__ __forceinline__ double team_dtlim(double tnext, double dtmax)
 // against this CTA's JL own predicted slots.  G lanes (a power of two)
 // share one i, each summing every G-th own slot, and their sums meet in a
 // fixed xor-shuffle tree; out(gi, f) is called by the first lane of each
-// group.  NW * 32 / G >= nr i-slots, nr <= kTeamIMax.
+// group.  NW * 32 / G >= nr i-slots, nr <= NW * 32.
 template <int ORDER, typename Idx, typename Out>
 __device__ __forceinline__ void team_force(const double *ibuf, const double *pred, int JL, int nr,
                                            double eps2, Idx idx, Out out)
@@ -128,12 +129,12 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
 {
     constexpr int T = kTeamWarps * 32;
     constexpr int R = Rec<ORDER>::words, F = Frc<ORDER>::words, P = Pred64<ORDER>::ncomp;
-    constexpr int IM = kTeamIMax;
     cg::cluster_group team = cg::this_cluster();
     const int C = (int)team.num_blocks(), rank = (int)team.block_rank();
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int jl_cap = L.jl_cap;
-    const int KM = IM / C;   // i states one rank pushes per step (its region of ibuf)
+    const int jl_cap = L.jl_cap;   // own slots per CTA
+    const int IM = L.im;           // i states per round (<= NW * 32)
+    const int KM = IM / C;         // i states one rank pushes per step (its region of ibuf)
 
     extern __shared__ __align__(16) unsigned char smem[];
     double *rec = reinterpret_cast<double *>(smem);               // [jl_cap][R] own records
@@ -209,6 +210,9 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
                 }
             }
             __syncwarp();
+            // the candidates' states predicted to m, pushed by one lane each
+            // into region `rank` of every CTA's ibuf (store instructions of
+            // one lane go to one rank back to back, from registers)
             const int kp = min(k, KM);
             for (int a = lane; a < kp; a += 32) {
                 const double *r = rec + (size_t)cand[a] * R;
@@ -410,11 +414,14 @@ cudaError_t team_setup_t(int ctas, TeamConfig *cfg)
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
-    const int avail = optin - 1024 - (int)(kTeamWarps * sizeof(double));   // static shared memory
-    int jl_cap = (int)((avail - (long long)TeamSmem<ORDER>::fixed) / (long long)TeamSmem<ORDER>::per_slot);
+    const int avail = optin - 1024;
+    // slots per CTA with the smallest round (kTeamIMax i-states)
+    using SM = TeamSmem<ORDER>;
+    int jl_cap = (int)(((long long)avail - (long long)SM::fixed - (long long)SM::per_i * kTeamIMax) /
+                       (long long)SM::per_slot);
     jl_cap = std::min(jl_cap & ~31, kTeamMaxSlotsPerCta);
     if (jl_cap < 32) return cudaErrorInvalidValue;
-    const int smem = (int)TeamSmem<ORDER>::bytes(jl_cap);
+    const int smem = avail;
     const void *k = (const void *)&team_kernel<ORDER>;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess && ctas > 8)
@@ -439,6 +446,27 @@ cudaError_t team_setup_t(int ctas, TeamConfig *cfg)
     cfg->smem = smem;
     cfg->max_teams = teams;
     return cudaSuccess;
+}
+
+// Launch shape for systems of up to nmax particles: the own slots per CTA
+// they need, and as many i-states per round (a multiple of 32, at most one
+// per thread) as the rest of the shared memory holds.
+template <int ORDER>
+int team_shape_t(const TeamConfig &cfg, int nmax, TeamLaunch *L)
+{
+    using SM = TeamSmem<ORDER>;
+    const int nch = (nmax + 31) / 32;
+    const int jl = (nch + cfg.ctas - 1) / cfg.ctas * 32;
+    if (jl > cfg.jl_cap) return -1;
+    long long im = ((long long)cfg.smem - (long long)SM::fixed - (long long)SM::per_slot * jl) /
+                   (long long)SM::per_i;
+    im = std::min<long long>(im & ~31LL, kTeamWarps * 32);
+    if (im < kTeamIMax) return -1;
+    L->ctas = cfg.ctas;
+    L->jl_cap = jl;
+    L->im = (int)im;
+    L->smem = (int)SM::bytes(jl, (int)im);
+    return 0;
 }
 
 template <int ORDER>
@@ -495,6 +523,16 @@ cudaError_t team_setup(int order, int ctas, TeamConfig *cfg)
     case 8: return team_setup_t<8>(ctas, cfg);
     }
     return cudaErrorInvalidValue;
+}
+
+int team_shape(int order, const TeamConfig &cfg, int nmax, TeamLaunch *L)
+{
+    switch (order) {
+    case 4: return team_shape_t<4>(cfg, nmax, L);
+    case 6: return team_shape_t<6>(cfg, nmax, L);
+    case 8: return team_shape_t<8>(cfg, nmax, L);
+    }
+    return -1;
 }
 
 cudaError_t team_launch(int order, const TeamLaunch &L, int teams, cudaStream_t s)
