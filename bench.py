@@ -430,8 +430,18 @@ def mixed_vs_fp64(dev, stream):
 def run_profile_case(case: str):
     """One small predict + two force launches, for ncu captures:
     fp64_o4 = the headline kernel (4th order FP64, N = 65536, all active);
-    mixed_o6 = 6th-order mixed precision, N = 65536, all active."""
+    mixed_o6 = 6th-order mixed precision, N = 65536, all active;
+    team_c1 = one team-kernel launch on c1 (N = 1024, 16 CTAs, t = 0..1/128)."""
     from hermite_b200 import Gravity
+    if case == "team_c1":
+        from hermite_b200.ic import plummer, records
+        with Gravity(4, 1024, "fp64") as g:
+            g.set_engine("team", 16)
+            g.set_jp_records(records(plummer(1024, 0), 4))
+            g.integrator_init(0.0, (1.0 / 256) ** 2, 0.01, 0.0025, 1.0 / 8)
+            g.integrator_run(1.0 / 128)
+            print("profile case team_c1 done", g.integrator_stats())
+        return
     order, prec = {"fp64_o4": (4, "fp64"), "mixed_o6": (6, "mixed"),
                    "fp64_o6": (6, "fp64"), "mixed_o8": (8, "mixed")}[case]
     g = Gravity(order, N, prec)
@@ -582,7 +592,7 @@ def main():
     ap.add_argument("--skip-mixed", action="store_true", help="omit the mixed-vs-FP64 leg")
     ap.add_argument("--skip-integrator", action="store_true",
                     help="omit the device-integrator block-step leg")
-    ap.add_argument("--profile", choices=("fp64_o4", "mixed_o6", "fp64_o6", "mixed_o8"),
+    ap.add_argument("--profile", choices=("fp64_o4", "mixed_o6", "fp64_o6", "mixed_o8", "team_c1"),
                     help="run one small case for an ncu capture and exit")
     args = ap.parse_args()
     if args.profile:
