@@ -684,10 +684,11 @@ int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double
     L.nsm = ctx->nsm;
     L.partial_cap = ctx->partial_cap;
     L.mixed = ctx->precision == HB_MIXED;
-    int smem = 0, per_sm = 0;
-    HB_CK(integrator_kernel_setup(ctx->order, L.mixed, &smem, &per_sm));
+    int smem = 0, per_sm = 0, big_per_sm = 0;
+    HB_CK(integrator_kernel_setup(ctx->order, L.mixed, &smem, &per_sm, &big_per_sm));
     L.smem_fp64 = L.smem_mixed = smem;
     L.items_grid = ctx->nsm * std::max(1, per_sm);
+    L.big_grid = ctx->nsm * std::max(1, big_per_sm);
     L.target_items = 2 * L.items_grid;
 
     if (ctx->stream == nullptr) return fail(ctx, HB_ERR_STATE, "integrator needs a non-default stream");
@@ -833,7 +834,7 @@ int hb_integrator_run(hb_ctx *ctx, double tend, long long max_block_steps)
             return fail(ctx, HB_ERR_STATE, "block-step limit %lld reached at t = %.17g",
                         max_block_steps, st->tsys);
         HB_CK(cudaGraphLaunch(ctx->int_exec, ctx->stream));
-        ctx->launches += 4LL * kStepsPerGraph;
+        ctx->launches += 5LL * kStepsPerGraph;
         s = sync_stream(ctx);
         if (s != HB_OK) return s;
         if (st->error)

@@ -27,6 +27,13 @@
 namespace hb {
 
 constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;   // +inf
+// Steps with more active slots than this use the large-step force kernel
+// (measured on N = 65536, 4th order: 512 and 2048 lose to the 32-slot items,
+// 4096 gains a few per cent).
+#ifndef HB_BIG_NACT
+#define HB_BIG_NACT 4096
+#endif
+constexpr int kBigNact = HB_BIG_NACT;
 
 // Programmatic dependent launch: let the next kernel of the step be
 // scheduled now, then wait until the previous kernel's results are visible.
@@ -109,6 +116,7 @@ struct ItemsArgs {
     int n, nchunk;
     size_t partial_cap;
     int target_items;
+    int big_nact;       // steps with more active slots take the large-step kernel
 };
 
 template <int ORDER, bool MIXED>
@@ -127,7 +135,7 @@ force_items_kernel(ItemsArgs a)
     __shared__ unsigned s_last;
 
     const int nact = a.s->nact;
-    if (nact == 0) return;
+    if (nact == 0 || nact > a.big_nact) return;   // large steps: force_items_big_kernel
     const double tsys = a.s->tnext, eps2 = a.s->eps2;
     const int tid = threadIdx.x, lane = tid & 31, jg = tid >> 5;
     const int gx = (nact + TI - 1) / TI;
@@ -236,6 +244,164 @@ force_items_kernel(ItemsArgs a)
             }
         }
         if (S > 1) {
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) s_last = (atomicAdd(&a.counter[itile], 1u) == (unsigned)(S - 1));
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                const int V = min(TI, nact - itile * TI) * F;
+                const double *pbase = a.partial + (size_t)itile * TI * F;
+                for (int e = tid; e < V; e += NW * 32) {
+                    double sum = 0.0;
+                    for (int s2 = 0; s2 < S; ++s2) sum += __ldcg(pbase + (size_t)s2 * ispan * F + e);
+                    a.force[(size_t)itile * TI * F + e] = sum;
+                }
+                if (tid == 0) a.counter[itile] = 0u;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// The same work for steps with many active slots: items of 4 warps x NI
+// i-chunks of 32 (NI = 2 at 4th order, 1 above, as the all-active tuning
+// chose), every warp over every j tile (no in-CTA j-split).  The raw
+// i-records fit the two stages of the j ring.
+template <int ORDER, bool MIXED>
+struct BigShape {
+    static constexpr int NW = 4, NI = ORDER == 4 ? 2 : 1, TCH = 4, STG = 2, TI = NW * NI * 32;
+    static constexpr int RB = Rec<ORDER>::bytes, CB = Layout<ORDER, MIXED>::chunk_bytes;
+    static constexpr int tile_bytes = TCH * 32 * RB;                 // one raw j stage
+    static constexpr int ring_bytes = STG * tile_bytes;
+    static constexpr int ptile_bytes = (TI / 32 > TCH ? TI / 32 : TCH) * CB;
+    static constexpr int smem_bytes = ring_bytes + ptile_bytes + 64;
+    static_assert(TI * RB <= ring_bytes, "the raw i-tile must fit the ring");
+};
+
+template <int ORDER, bool MIXED>
+__global__ void __launch_bounds__(128)
+force_items_big_kernel(ItemsArgs a)
+{
+    pdl_enter();
+    using B = BigShape<ORDER, MIXED>;
+    constexpr int NW = B::NW, NI = B::NI, TCH = B::TCH, STG = B::STG, TI = B::TI, CB = B::CB;
+    constexpr int F = Frc<ORDER>::words, R = Rec<ORDER>::words, RB = Rec<ORDER>::bytes;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + B::ring_bytes + B::ptile_bytes);
+    unsigned char *ptile = smem + B::ring_bytes;
+    __shared__ int s_item;
+    __shared__ unsigned s_last;
+
+    const int nact = a.s->nact;
+    if (nact <= a.big_nact) return;
+    const double tsys = a.s->tnext, eps2 = a.s->eps2;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gx = (nact + TI - 1) / TI;
+    int S = (a.target_items + gx - 1) / gx;
+    S = max(1, min(S, max(1, a.nchunk / 8)));
+    while (S > 1 && (size_t)S * gx * TI * F > a.partial_cap) --S;
+    const int items = gx * S;
+    const size_t ispan = (size_t)gx * TI;
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    unsigned g = 0;   // tiles issued by this CTA so far (mbarrier phases)
+    const float2 eps2f = f2((float)eps2);
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(&a.s->work, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= items) break;
+        const int itile = item / S, sl = item % S;
+
+        // gather the TI i-records of this tile into the ring, predict them
+        double *raw = reinterpret_cast<double *>(smem);
+        for (int w = tid; w < TI * R; w += NW * 32) {
+            const int q = w / R, k = itile * TI + q;
+            const int slot = a.ilist[k < nact ? k : nact - 1];
+            raw[w] = a.jp[(size_t)slot * R + (w - q * R)];
+        }
+        __syncthreads();
+        predict_tile<ORDER, MIXED>(raw, TI, 0, 0x7fffffff, tsys, ptile);
+        __syncthreads();
+        using IBody = typename std::conditional<MIXED, NegI32, Body64>::type;
+        IBody I[NI];
+#pragma unroll
+        for (int n = 0; n < NI; ++n) {
+            if constexpr (MIXED) load_i_mixed<ORDER>(reinterpret_cast<const float *>(ptile), warp * NI + n, lane, I[n]);
+            else load_i64<ORDER>(reinterpret_cast<const double *>(ptile), warp * NI + n, lane, I[n]);
+        }
+        __syncthreads();
+
+        double f[NI][F];
+#pragma unroll
+        for (int n = 0; n < NI; ++n)
+#pragma unroll
+            for (int c = 0; c < F; ++c) f[n][c] = 0.0;
+        const int c0 = (int)(((long long)sl * a.nchunk) / S);
+        const int c1 = (int)(((long long)(sl + 1) * a.nchunk) / S);
+        const int ntile = (c1 - c0 + TCH - 1) / TCH;
+        auto issue = [&](int t) {
+            const unsigned gt = g + t;
+            const int st = gt % STG;
+            const int cs = c0 + t * TCH, cnt = min(TCH, c1 - cs);
+            const uint32_t bytes = (uint32_t)(cnt * 32 * RB);
+            mbar_arrive_expect_tx(&bar[st], bytes);
+            bulk_load(smem + st * B::tile_bytes, a.jp + (size_t)cs * 32 * R, bytes, &bar[st]);
+        };
+        if (tid == 0)
+            for (int t = 0; t < STG && t < ntile; ++t) issue(t);
+        int failed_at = -1;
+        for (int t = 0; t < ntile; ++t) {
+            const unsigned gt = g + t;
+            const int st = gt % STG;
+            const bool got = mbar_wait_bounded(&bar[st], (gt / STG) & 1u);
+            if (!__syncthreads_and(got)) { failed_at = t; break; }
+            const int cnt = min(TCH, c1 - (c0 + t * TCH));
+            predict_tile<ORDER, MIXED>(reinterpret_cast<const double *>(smem + st * B::tile_bytes),
+                                       cnt * 32, (c0 + t * TCH) * 32, a.n, tsys, ptile);
+            __syncthreads();
+            if (tid == 0 && t + STG < ntile) issue(t + STG);
+            for (int q = 0; q < cnt; ++q) {
+                if constexpr (MIXED)
+                    chunk_mixed<ORDER, NI, (HB_MIXED_REFINE != 0)>(reinterpret_cast<const float *>(ptile + q * CB), I, eps2f, f);
+                else
+                    chunk64<ORDER, NI>(reinterpret_cast<const double *>(ptile + q * CB), I, eps2, f);
+            }
+            __syncthreads();
+        }
+        if (failed_at >= 0) {
+            if (tid == 0) {
+                raise_error(a.err, kErrWaitTimeout);
+                for (int t = failed_at; t < ntile && t < failed_at + STG; ++t)
+                    mbar_wait_bounded(&bar[(g + t) % STG], ((g + t) / STG) & 1u);
+            }
+            a.s->error = 2;
+            return;
+        }
+        g += ntile;
+
+        if (S == 1) {
+#pragma unroll
+            for (int n = 0; n < NI; ++n) {
+                const int k = itile * TI + (warp * NI + n) * 32 + lane;
+                if (k < nact)
+#pragma unroll
+                    for (int c = 0; c < F; ++c) a.force[(size_t)k * F + c] = f[n][c];
+            }
+        } else {
+#pragma unroll
+            for (int n = 0; n < NI; ++n) {
+                const int k = itile * TI + (warp * NI + n) * 32 + lane;
+#pragma unroll
+                for (int c = 0; c < F; ++c) a.partial[((size_t)sl * ispan + k) * F + c] = f[n][c];
+            }
             __threadfence();
             __syncthreads();
             if (tid == 0) s_last = (atomicAdd(&a.counter[itile], 1u) == (unsigned)(S - 1));
@@ -375,12 +541,22 @@ static cudaError_t launch_step(const IntegratorLaunch &L, cudaStream_t s)
         e = launch_pdl(sched_compact_kernel<ORDER>, nb, 256, 0, s, (const double *)L.jp,
                        (const double *)L.dt, L.n, L.sched, L.ilist);
     ItemsArgs a{L.jp, L.ilist, L.sched, L.force, L.partial, L.counter, L.err, L.n, L.nchunk,
-                L.partial_cap, L.target_items};
+                L.partial_cap, L.target_items, kBigNact};
+    // both force shapes are in every step; the one not meant for this step's
+    // nact (known on the device only) returns at once
     if (e == cudaSuccess) {
         if (L.mixed)
             e = launch_pdl(force_items_kernel<ORDER, true>, L.items_grid, 128, L.smem_mixed, s, a);
         else
             e = launch_pdl(force_items_kernel<ORDER, false>, L.items_grid, 128, L.smem_fp64, s, a);
+    }
+    if (e == cudaSuccess) {
+        if (L.mixed)
+            e = launch_pdl(force_items_big_kernel<ORDER, true>, L.big_grid, 128,
+                           BigShape<ORDER, true>::smem_bytes, s, a);
+        else
+            e = launch_pdl(force_items_big_kernel<ORDER, false>, L.big_grid, 128,
+                           BigShape<ORDER, false>::smem_bytes, s, a);
     }
     if (e == cudaSuccess)
         e = launch_pdl(correct_kernel<ORDER>, std::max(1, std::min(nb, L.nsm * 4)), 256, 0, s, L.jp,
@@ -398,7 +574,8 @@ cudaError_t integrator_step_launch(int order, const IntegratorLaunch &L, cudaStr
     return cudaErrorInvalidValue;
 }
 
-cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *grid_per_sm)
+cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *grid_per_sm,
+                                    int *big_per_sm)
 {
     const void *k = nullptr;
     int sm = 0;
@@ -418,7 +595,24 @@ cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *grid_
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
     *smem = sm;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(grid_per_sm, k, 128, sm);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(grid_per_sm, k, 128, sm);
+    if (e != cudaSuccess) return e;
+    // the large-step kernel
+#define HB_BIG(O, M)                                                                          \
+    k = (const void *)&force_items_big_kernel<O, M>;                                            \
+    sm = BigShape<O, M>::smem_bytes;
+    switch (order * 2 + (mixed ? 1 : 0)) {
+    case 8: HB_BIG(4, false) break;
+    case 9: HB_BIG(4, true) break;
+    case 12: HB_BIG(6, false) break;
+    case 13: HB_BIG(6, true) break;
+    case 16: HB_BIG(8, false) break;
+    default: HB_BIG(8, true) break;
+    }
+#undef HB_BIG
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(big_per_sm, k, 128, sm);
 }
 
 cudaError_t integrator_assign(int order, double *jp, double *dt, const double *force, int n,

@@ -66,6 +66,7 @@ struct IntegratorLaunch {
     int n, nchunk, nsm;
     size_t partial_cap;
     int target_items, items_grid, smem_fp64, smem_mixed;
+    int big_grid;       // grid of the large-step force kernel
     bool mixed;
 };
 
@@ -110,7 +111,8 @@ int team_shape(int order, const TeamConfig &cfg, int nmax, TeamLaunch *L);
 cudaError_t team_launch(int order, const TeamLaunch &L, int teams, cudaStream_t s);
 cudaError_t team_sched_sync(Sched *s, TeamState *st, bool to_team, cudaStream_t stream);
 
-cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *blocks_per_sm);
+cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *blocks_per_sm,
+                                    int *big_per_sm);
 cudaError_t integrator_assign(int order, double *jp, double *dt, const double *force, int n,
                               int set_dt, double eta_s, double dtmax, cudaStream_t s);
 cudaError_t integrator_energy(int order, const double *jp, const double *pot, int n, double *part,

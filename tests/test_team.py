@@ -42,6 +42,8 @@ def integrate(order, n, engine, ctas=0, tend=1.0 / 8, seed=3, eta=None):
     (4, 40, 4),            # 2 chunks over 4 CTAs: two CTAs own nothing
     (6, 33, 2),
     (4, 3000, 0),          # first steps have > 256 active slots: several rounds
+    (6, 4500, 0),          # steps with > 4096 active slots: the graph engine's large-step kernel
+    (8, 4200, 0),
 ])
 def test_team_matches_graph_engine(order, n, ctas):
     s_g, rec_g, dt_g, used_g = integrate(order, n, "graph")
