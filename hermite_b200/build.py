@@ -28,7 +28,7 @@ LIB = LIBDIR / "libhermite_b200.so"
 INCLUDE = ROOT / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fopenmp",
               "--expt-relaxed-constexpr", "-I", str(INCLUDE), "-I", str(CSRC)]
 SOURCES = ["hb_capi.cu", "hb_predict_pot.cu", "hb_force_64.cu", "hb_force_mixed.cu",
            "hb_noalloc.cu", "hb_integrator.cu", "hb_ensemble.cu", "hb_team.cu"]
@@ -76,7 +76,8 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) 
     objs = [BUILD / (Path(s).stem + ".o") for s in SOURCES]
     if force or jobs or _stale(LIB, objs):
         tmp = LIB.with_suffix(".so.tmp")
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-cudart", "static"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-cudart", "static",
+               "-Xcompiler", "-fopenmp"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

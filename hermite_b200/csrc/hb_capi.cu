@@ -30,9 +30,11 @@ using namespace hb;
 
 namespace {
 constexpr int kMaxBody = 1 << 24;
+// hb_set_jp_records of at least this many bytes uploads at once, in chunks.
+constexpr size_t kEagerUploadBytes = (size_t)4 << 20, kUploadChunkBytes = (size_t)2 << 20;
 // HB_ENGINE_AUTO takes the team engine up to this many particles.
 constexpr int kTeamAutoMaxBody = 3072;
-constexpr int kNumVariants = 18;
+constexpr int kNumVariants = 20;
 
 int rec_words(int order) { return 8 + 3 * (order - 2); }
 int force_words(int order) { return 3 * (order / 2); }
@@ -122,6 +124,26 @@ void mark_dirty(hb_ctx *c, int lo, int hi)
 void wait_upload(hb_ctx *c)
 {
     if (c->upload_pending.load(std::memory_order_acquire)) cudaEventSynchronize(c->ev_upload);
+}
+
+// Host copies of megabytes (bulk records in, forces and potentials out) are
+// memory-bandwidth work: split over up to 8 host threads.
+void host_copy(void *dst, const void *src, size_t bytes)
+{
+    constexpr size_t kParallel = (size_t)1 << 20, kPerThread = (size_t)256 << 10;
+    if (bytes < kParallel) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const int nt = (int)std::min<size_t>(8, bytes / kPerThread);
+    const size_t per = (bytes + nt - 1) / nt;
+#pragma omp parallel for num_threads(nt) schedule(static, 1)
+    for (int t = 0; t < nt; ++t) {
+        const size_t o = (size_t)t * per;
+        if (o < bytes)
+            std::memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o,
+                        std::min(per, bytes - o));
+    }
 }
 
 int do_upload(hb_ctx *ctx)
@@ -431,9 +453,25 @@ int hb_set_jp_records(hb_ctx *ctx, int addr0, int count, const double *records)
         return HB_ERR_INVALID;
     if (count == 0) return HB_OK;
     wait_upload(ctx);
-    std::memcpy(ctx->h_jp + (size_t)addr0 * ctx->R, records,
-                sizeof(double) * (size_t)count * ctx->R);
-    mark_dirty(ctx, addr0, addr0 + count);
+    const size_t off = (size_t)addr0 * ctx->R, bytes = sizeof(double) * (size_t)count * ctx->R;
+    if (bytes < kEagerUploadBytes) {
+        host_copy(ctx->h_jp + off, records, bytes);
+        mark_dirty(ctx, addr0, addr0 + count);
+        return HB_OK;
+    }
+    // A bulk set: copy into the pinned mirror chunk by chunk and upload each
+    // chunk while the next one is copied (stream-ordered after any force
+    // still reading the device copy).  These slots need no later upload.
+    const char *src = reinterpret_cast<const char *>(records);
+    char *hm = reinterpret_cast<char *>(ctx->h_jp + off);
+    char *dm = reinterpret_cast<char *>(ctx->d_jp + off);
+    for (size_t o = 0; o < bytes; o += kUploadChunkBytes) {
+        const size_t len = std::min(kUploadChunkBytes, bytes - o);
+        host_copy(hm + o, src + o, len);
+        HB_CK(cudaMemcpyAsync(dm + o, hm + o, len, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    HB_CK(cudaEventRecord(ctx->ev_upload, ctx->stream));
+    ctx->upload_pending.store(true, std::memory_order_release);
     return HB_OK;
 }
 
@@ -482,7 +520,7 @@ int hb_download_forces(hb_ctx *ctx, int nact, double *force_out)
     }
     int s = sync_stream(ctx);
     if (s != HB_OK) return s;
-    if (nact > 0) std::memcpy(force_out, ctx->h_force, sizeof(double) * (size_t)nact * ctx->F);
+    if (nact > 0) host_copy(force_out, ctx->h_force, sizeof(double) * (size_t)nact * ctx->F);
     return HB_OK;
 }
 
@@ -526,7 +564,7 @@ int hb_potential(hb_ctx *ctx, double eps2, double *pot_out)
                           cudaMemcpyDeviceToHost, ctx->stream));
     s = sync_stream(ctx);
     if (s != HB_OK) return s;
-    std::memcpy(pot_out, ctx->h_pot, sizeof(double) * ctx->nbody);
+    host_copy(pot_out, ctx->h_pot, sizeof(double) * ctx->nbody);
     return HB_OK;
 }
 

@@ -28,9 +28,12 @@ ForceVariant make_variant()
 // Fused predict + force (each CTA predicts the raw records it streams):
 //  12: as 0    13: as 2    14: as 3    15: as 8    16: as 1 with 8-chunk tiles
 //  17: as 5
+// Two-pass, 2 i-chunks per warp (appended):
+//  18: 2 warps, 2 i-chunks/warp                        (128 i per CTA)
+//  19: as 1 with 8-chunk tiles
 template <int ORDER, bool MIXED>
 struct VariantTable {
-    static constexpr int count = 18;
+    static constexpr int count = 20;
     ForceVariant v[count];
     VariantTable()
         : v{make_variant<ORDER, MIXED, 4, 1, 1, 4>(),
@@ -50,7 +53,9 @@ struct VariantTable {
             make_variant<ORDER, MIXED, 4, 1, 2, 4, 0, true>(),
             make_variant<ORDER, MIXED, 2, 1, 1, 4, 8, true>(),
             make_variant<ORDER, MIXED, 4, 2, 1, 8, 0, true>(),
-            make_variant<ORDER, MIXED, 4, 1, 1, 4, 5, true>()} {}
+            make_variant<ORDER, MIXED, 4, 1, 1, 4, 5, true>(),
+            make_variant<ORDER, MIXED, 2, 2, 1, 4>(),
+            make_variant<ORDER, MIXED, 4, 2, 1, 8>()} {}
 };
 
 }  // namespace hb

@@ -63,7 +63,7 @@ def test_mixed_partial_nact(order, nact, oracle):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("variant", list(range(18)))
+@pytest.mark.parametrize("variant", list(range(20)))
 @pytest.mark.parametrize("jsplit", [1, 3, 16])
 def test_every_launch_shape(precision, variant, jsplit, oracle):
     _check(6, 2500, 700, precision, oracle, seed=11, variant=variant, jsplit=jsplit)
