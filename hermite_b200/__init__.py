@@ -50,7 +50,8 @@ EXPORTED_SYMBOLS = (
     "hb_get_records", "hb_ens_create", "hb_ens_destroy", "hb_ens_last_error",
     "hb_ens_set_cluster", "hb_ens_get_cluster", "hb_ens_cluster_offset", "hb_ens_init",
     "hb_ens_run", "hb_ens_stats", "hb_ens_energy", "hb_ens_set_engine", "hb_ens_cluster_engine",
-    "hb_ens_cluster_stats",
+    "hb_ens_cluster_stats", "hb_dump_write", "hb_dump_read_header", "hb_dump_read",
+    "hb_integrator_dump", "hb_integrator_restore",
 )
 
 
@@ -63,6 +64,50 @@ def record_words(order: int) -> int:
 
 def force_words(order: int) -> int:
     return 3 * (order // 2)
+
+
+AUX_WORDS = 6    # per particle: snp crk (4th), d4a d5a (6th), d6a d7a (8th)
+
+
+def write_dump(path, order: int, records, aux, tsys: float, dumpid: int = 0,
+               energies=(0.0, 0.0), steps=(0, 0), ids=None):
+    """Write a checkpoint in the reference's dump format (host only)."""
+    lib = load_library()
+    rec = np.ascontiguousarray(records, dtype=np.float64).reshape(-1, record_words(order))
+    ax = np.ascontiguousarray(aux, dtype=np.float64).reshape(rec.shape[0], AUX_WORDS)
+    idp = None
+    if ids is not None:
+        idarr = np.ascontiguousarray(ids, dtype=np.int64)
+        idp = idarr.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
+    st = lib.hb_dump_write(str(path).encode(), int(order), int(dumpid), rec.shape[0], float(tsys),
+                           float(energies[0]), float(energies[1]), int(steps[0]), int(steps[1]),
+                           idp, _dptr(rec), _dptr(ax))
+    if st != 0:
+        raise HermiteError(st, f"hb_dump_write {path}: " + lib.hb_status_string(st).decode())
+
+
+def read_dump(path) -> dict:
+    """Read a checkpoint in the reference's dump format (host only): header
+    fields, ids, records (tlast = tsys) and the aux derivatives."""
+    lib = load_library()
+    o, d, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    t, e0, e1 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    ps, bs = ctypes.c_longlong(), ctypes.c_longlong()
+    st = lib.hb_dump_read_header(str(path).encode(), ctypes.byref(o), ctypes.byref(d),
+                                 ctypes.byref(n), ctypes.byref(t), ctypes.byref(e0),
+                                 ctypes.byref(e1), ctypes.byref(ps), ctypes.byref(bs))
+    if st != 0:
+        raise HermiteError(st, f"hb_dump_read_header {path}: " + lib.hb_status_string(st).decode())
+    rec = np.empty((n.value, record_words(o.value)))
+    aux = np.empty((n.value, AUX_WORDS))
+    ids = np.empty(n.value, dtype=np.int64)
+    st = lib.hb_dump_read(str(path).encode(), o.value, n.value,
+                          ids.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), _dptr(rec), _dptr(aux))
+    if st != 0:
+        raise HermiteError(st, f"hb_dump_read {path}: " + lib.hb_status_string(st).decode())
+    return {"order": o.value, "dumpid": d.value, "nbody": n.value, "tsys": t.value,
+            "energies": (e0.value, e1.value), "steps": (ps.value, bs.value), "ids": ids,
+            "records": rec, "aux": aux}
 
 
 class HermiteError(RuntimeError):
@@ -135,6 +180,15 @@ def load_library() -> ctypes.CDLL:
         "hb_ens_cluster_engine": (I, [P, I, ctypes.POINTER(I), ctypes.POINTER(I)]),
         "hb_ens_cluster_stats": (I, [P, I, ctypes.POINTER(ctypes.c_longlong),
                                      ctypes.POINTER(ctypes.c_longlong), dp]),
+        "hb_dump_write": (I, [ctypes.c_char_p, I, I, I, D, D, D, ctypes.c_longlong,
+                              ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong), dp, dp]),
+        "hb_dump_read_header": (I, [ctypes.c_char_p, ctypes.POINTER(I), ctypes.POINTER(I),
+                                    ctypes.POINTER(I), dp, dp, dp,
+                                    ctypes.POINTER(ctypes.c_longlong),
+                                    ctypes.POINTER(ctypes.c_longlong)]),
+        "hb_dump_read": (I, [ctypes.c_char_p, I, I, ctypes.POINTER(ctypes.c_longlong), dp, dp]),
+        "hb_integrator_dump": (I, [P, ctypes.c_char_p, I, D, D]),
+        "hb_integrator_restore": (I, [P, ctypes.c_char_p, D, D, D, ctypes.POINTER(I), dp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -292,6 +346,25 @@ class Gravity:
         self._check(self._lib.hb_integrator_stats(self._h, ctypes.byref(ps), ctypes.byref(bs),
                                                   ctypes.byref(t)), "integrator_stats")
         return ps.value, bs.value, t.value
+
+    def integrator_dump(self, path, dumpid: int = 0, init_energy: float = 0.0,
+                        prev_energy: float = 0.0):
+        """Checkpoint the device integrator in the reference's dump format
+        (every particle must be at the block time: a multiple of dtmax)."""
+        self._check(self._lib.hb_integrator_dump(self._h, str(path).encode(), int(dumpid),
+                                                 float(init_energy), float(prev_energy)),
+                    "integrator_dump")
+
+    def integrator_restore(self, path, eps2: float, eta: float, dtmax: float):
+        """Restore a dump (ours or the reference's) and prepare the integrator
+        as the reference's restore + reinitialize_steps; returns (dumpid,
+        initial energy, previous energy)."""
+        d, e0, e1 = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        self._check(self._lib.hb_integrator_restore(self._h, str(path).encode(), float(eps2),
+                                                    float(eta), float(dtmax), ctypes.byref(d),
+                                                    ctypes.byref(e0), ctypes.byref(e1)),
+                    "integrator_restore")
+        return d.value, e0.value, e1.value
 
     def energy(self, eps2: float):
         ke, pe = ctypes.c_double(), ctypes.c_double()

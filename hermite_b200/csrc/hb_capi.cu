@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "hermite_b200.h"
 #include "hb_common.cuh"
@@ -82,6 +83,7 @@ struct hb_ctx {
     // team engine (hb_team.cu)
     int engine = HB_ENGINE_AUTO, team_ctas = 0;
     TeamSys *d_team_sys = nullptr;
+    double *d_aux = nullptr;          // per-slot dump derivatives
     TeamState *d_team_state = nullptr;
     int *d_team_next = nullptr;
     int blocks_per_sm[2][kNumVariants] = {};
@@ -317,6 +319,7 @@ const char *hb_status_string(int s)
     case HB_ERR_NO_DEVICE: return "no sm_100 CUDA device";
     case HB_ERR_STATE: return "call out of order";
     case HB_ERR_TOO_LARGE: return "size exceeds a fixed capacity";
+    case HB_ERR_IO: return "file could not be written or parsed";
     }
     return "unknown status";
 }
@@ -353,6 +356,7 @@ int hb_destroy(hb_ctx *ctx)
     cudaFree(ctx->d_ilist);
     cudaFree(ctx->d_epart);
     cudaFree(ctx->d_team_sys);
+    cudaFree(ctx->d_aux);
     cudaFree(ctx->d_team_state);
     cudaFree(ctx->d_team_next);
     if (ctx->ev_upload) cudaEventDestroy(ctx->ev_upload);
@@ -643,6 +647,7 @@ int integrator_alloc(hb_ctx *ctx)
               cudaMalloc((void **)&ctx->d_dt, np * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_ilist, np * sizeof(int)) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_epart, 2 * kEnergyParts * sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void **)&ctx->d_aux, np * kAuxWords * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_team_sys, sizeof(TeamSys)) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_team_state, sizeof(TeamState)) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_team_next, sizeof(int)) == cudaSuccess;
@@ -655,44 +660,12 @@ int integrator_alloc(hb_ctx *ctx)
 }
 }  // namespace
 
-int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double eta_s, double dtmax)
+namespace {
+// Scheduler state and the captured block-step graph for the records, dt and
+// dump derivatives now on the device (after init_step or a restore).
+int setup_integrator(hb_ctx *ctx, double tsys, double eps2, double eta, double dtmax,
+                     long long particle_steps, long long block_steps)
 {
-    if (!ctx) return HB_ERR_INVALID;
-    if (!(eps2 >= 0.0) || !(eta > 0.0) || !(eta_s > 0.0) || !(dtmax > 0.0) ||
-        std::log2(dtmax) != std::floor(std::log2(dtmax)) || !(tsys >= 0.0))
-        return fail(ctx, HB_ERR_INVALID, "integrator_init: need eps2 >= 0, eta, eta_s > 0, "
-                                         "dtmax a power of two, tsys >= 0");
-    int s = integrator_alloc(ctx);
-    if (s != HB_OK) return s;
-    s = sync_stream(ctx);
-    if (s != HB_OK) return s;
-    if (ctx->int_exec) { cudaGraphExecDestroy(ctx->int_exec); ctx->int_exec = nullptr; }
-    if (ctx->int_graph) { cudaGraphDestroy(ctx->int_graph); ctx->int_graph = nullptr; }
-    ctx->int_ready = false;
-
-    // initial conditions: the mirror's pos, mass, vel at tlast = tsys, all
-    // derivatives zero (the reference's Particle constructor), as in
-    // NbodySystem::init_step (SRC/nbodysystem.h:565-631)
-    for (int i = 0; i < ctx->nbody; ++i) {
-        double *r = ctx->h_jp + (size_t)i * ctx->R;
-        r[7] = tsys;
-        std::memset(r + 8, 0, sizeof(double) * (ctx->R - 8));
-    }
-    mark_dirty(ctx, 0, ctx->nbody);
-    s = do_upload(ctx);
-    if (s != HB_OK) return s;
-    const int passes = ctx->order > 4 ? 2 : 1;   // higher derivatives bootstrap
-    for (int p = 0; p < passes; ++p) {
-        hb_predict_all_device(ctx, tsys);
-        s = run_force(ctx, ctx->nbody, eps2, ctx->d_force);
-        if (s != HB_OK) return s;
-        HB_CK(integrator_assign(ctx->order, ctx->d_jp, ctx->d_dt, ctx->d_force, ctx->nbody,
-                                p == passes - 1, eta_s, dtmax, ctx->stream));
-        ctx->launches++;
-    }
-    s = sync_stream(ctx);
-    if (s != HB_OK) return s;
-
     Sched &sc = *ctx->h_sched;
     std::memset(&sc, 0, sizeof(Sched));
     sc.tnext_bits = 0x7ff0000000000000ull;
@@ -701,9 +674,13 @@ int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double
     sc.eps2 = eps2;
     sc.etapow = std::pow(eta, 2.0 * (ctx->order - 3));   // set_run_params, SRC/nbodysystem.h:472
     sc.dtmax = dtmax;
+    sc.particle_steps = particle_steps;
+    sc.block_steps = block_steps;
     sc.status = ctx->d_status;
     std::memset(ctx->h_status, 0, sizeof(IntStatus));
     ctx->h_status->tsys = tsys;
+    ctx->h_status->particle_steps = particle_steps;
+    ctx->h_status->block_steps = block_steps;
     HB_CK(cudaMemcpy(ctx->d_sched, &sc, sizeof(Sched), cudaMemcpyHostToDevice));
     const TeamSys ts{0, ctx->nbody, 0, eps2};
     HB_CK(cudaMemcpy(ctx->d_team_sys, &ts, sizeof(TeamSys), cudaMemcpyHostToDevice));
@@ -711,6 +688,7 @@ int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double
     IntegratorLaunch L;
     L.jp = ctx->d_jp;
     L.dt = ctx->d_dt;
+    L.aux = ctx->d_aux;
     L.ilist = ctx->d_ilist;
     L.sched = ctx->d_sched;
     L.force = ctx->d_force;
@@ -746,6 +724,121 @@ int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double
     ctx->int_ready = true;
     ctx->pred_precision = ctx->precision;
     return HB_OK;
+}
+
+int reset_integrator(hb_ctx *ctx)
+{
+    int s = integrator_alloc(ctx);
+    if (s == HB_OK) s = sync_stream(ctx);
+    if (s != HB_OK) return s;
+    if (ctx->int_exec) { cudaGraphExecDestroy(ctx->int_exec); ctx->int_exec = nullptr; }
+    if (ctx->int_graph) { cudaGraphDestroy(ctx->int_graph); ctx->int_graph = nullptr; }
+    ctx->int_ready = false;
+    return HB_OK;
+}
+
+bool power_of_two(double x) { return x > 0.0 && std::log2(x) == std::floor(std::log2(x)); }
+}  // namespace
+
+int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double eta_s, double dtmax)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    if (!(eps2 >= 0.0) || !(eta > 0.0) || !(eta_s > 0.0) || !power_of_two(dtmax) || !(tsys >= 0.0))
+        return fail(ctx, HB_ERR_INVALID, "integrator_init: need eps2 >= 0, eta, eta_s > 0, "
+                                         "dtmax a power of two, tsys >= 0");
+    int s = reset_integrator(ctx);
+    if (s != HB_OK) return s;
+
+    // initial conditions: the mirror's pos, mass, vel at tlast = tsys, all
+    // derivatives zero (the reference's Particle constructor), as in
+    // NbodySystem::init_step (SRC/nbodysystem.h:565-631)
+    for (int i = 0; i < ctx->nbody; ++i) {
+        double *r = ctx->h_jp + (size_t)i * ctx->R;
+        r[7] = tsys;
+        std::memset(r + 8, 0, sizeof(double) * (ctx->R - 8));
+    }
+    mark_dirty(ctx, 0, ctx->nbody);
+    s = do_upload(ctx);
+    if (s != HB_OK) return s;
+    HB_CK(cudaMemsetAsync(ctx->d_aux, 0, sizeof(double) * ctx->npad * kAuxWords, ctx->stream));
+    const int passes = ctx->order > 4 ? 2 : 1;   // higher derivatives bootstrap
+    for (int p = 0; p < passes; ++p) {
+        hb_predict_all_device(ctx, tsys);
+        s = run_force(ctx, ctx->nbody, eps2, ctx->d_force);
+        if (s != HB_OK) return s;
+        HB_CK(integrator_assign(ctx->order, ctx->d_jp, ctx->d_dt, ctx->d_force, ctx->nbody,
+                                p == passes - 1, eta_s, dtmax, ctx->stream));
+        ctx->launches++;
+    }
+    s = sync_stream(ctx);
+    if (s != HB_OK) return s;
+    return setup_integrator(ctx, tsys, eps2, eta, dtmax, 0, 0);
+}
+
+int hb_integrator_dump(hb_ctx *ctx, const char *path, int dumpid, double init_energy,
+                       double prev_energy)
+{
+    if (!ctx || !path) return HB_ERR_INVALID;
+    if (!ctx->int_ready) return fail(ctx, HB_ERR_STATE, "hb_integrator_dump before hb_integrator_init");
+    int s = sync_stream(ctx);
+    if (s != HB_OK) return s;
+    const size_t n = ctx->nbody;
+    std::vector<double> rec(n * ctx->R), aux(n * kAuxWords);
+    HB_CK(cudaMemcpy(rec.data(), ctx->d_jp, rec.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    HB_CK(cudaMemcpy(aux.data(), ctx->d_aux, aux.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    const volatile IntStatus *st = ctx->h_status;
+    const double tsys = st->tsys;
+    for (size_t i = 0; i < n; ++i)
+        if (rec[i * ctx->R + 7] != tsys)
+            return fail(ctx, HB_ERR_STATE, "dump at t = %.17g: slot %zu is at %.17g (dump at a multiple "
+                                           "of dtmax, where every particle is at the block time)",
+                        tsys, i, rec[i * ctx->R + 7]);
+    s = hb_dump_write(path, ctx->order, dumpid, ctx->nbody, tsys, init_energy, prev_energy,
+                      st->particle_steps, st->block_steps, nullptr, rec.data(), aux.data());
+    return s == HB_OK ? HB_OK : fail(ctx, s, "cannot write the dump file %s", path);
+}
+
+int hb_integrator_restore(hb_ctx *ctx, const char *path, double eps2, double eta, double dtmax,
+                          int *dumpid, double *init_energy, double *prev_energy)
+{
+    if (!ctx || !path) return HB_ERR_INVALID;
+    if (!(eps2 >= 0.0) || !(eta > 0.0) || !power_of_two(dtmax))
+        return fail(ctx, HB_ERR_INVALID, "integrator_restore: need eps2 >= 0, eta > 0, dtmax a power of two");
+    int order = 0, did = 0, nb = 0;
+    double tsys = 0.0, e0 = 0.0, e1 = 0.0;
+    long long steps = 0, bsteps = 0;
+    int s = hb_dump_read_header(path, &order, &did, &nb, &tsys, &e0, &e1, &steps, &bsteps);
+    if (s != HB_OK) return fail(ctx, s, "cannot read the dump header of %s", path);
+    if (order != ctx->order || nb != ctx->nbody)
+        return fail(ctx, HB_ERR_INVALID, "the dump holds order %d, N = %d; the context order %d, N = %d",
+                    order, nb, ctx->order, ctx->nbody);
+    s = reset_integrator(ctx);
+    if (s != HB_OK) return s;
+    const size_t n = nb;
+    std::vector<double> rec(n * ctx->R), aux(n * kAuxWords), dt(n);
+    s = hb_dump_read(path, order, nb, nullptr, rec.data(), aux.data());
+    if (s != HB_OK) return fail(ctx, s, "cannot read the dump particles of %s", path);
+    // NbodySystem::restore + reinitialize_steps (SRC/nbodysystem.h:429-458):
+    // tlast = tsys, dt from recalc_dt
+    for (size_t i = 0; i < n; ++i) {
+        rec[i * ctx->R + 7] = tsys;
+        dt[i] = recalc_dt(order, rec.data() + i * ctx->R, aux.data() + i * kAuxWords, eta, dtmax);
+    }
+    wait_upload(ctx);
+    std::memcpy(ctx->h_jp, rec.data(), rec.size() * sizeof(double));
+    mark_dirty(ctx, 0, nb);
+    s = do_upload(ctx);
+    if (s != HB_OK) return s;
+    HB_CK(cudaMemcpyAsync(ctx->d_aux, aux.data(), aux.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          ctx->stream));
+    HB_CK(cudaMemcpyAsync(ctx->d_dt, dt.data(), dt.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          ctx->stream));
+    s = sync_stream(ctx);
+    if (s != HB_OK) return s;
+    if (dumpid) *dumpid = did;
+    if (init_energy) *init_energy = e0;
+    if (prev_energy) *prev_energy = e1;
+    return setup_integrator(ctx, tsys, eps2, eta, dtmax, steps, bsteps);
 }
 
 namespace {
@@ -796,6 +889,7 @@ int run_team(hb_ctx *ctx, const TeamConfig &cfg, double tend, long long max_bloc
     TeamLaunch L;
     L.jp = ctx->d_jp;
     L.dt = ctx->d_dt;
+    L.aux = ctx->d_aux;
     L.sys = ctx->d_team_sys;
     L.st = ctx->d_team_state;
     L.next_sys = ctx->d_team_next;

@@ -47,10 +47,12 @@ __device__ __forceinline__ double norm2(V3 a)
 
 // Particle state in a j-particle record r (pos mass vel tlast acc jrk [snp
 // crk] [d4a d5a]); f = the new force (acc jrk [snp] [crk]).  Returns the new
-// dt; writes the corrected state into r.
+// dt; writes the corrected state into r.  If aux is not null it receives the
+// two higher derivatives the reference's Particle also keeps and dumps (snp
+// crk at 4th order, d4a d5a at 6th, d6a d7a at 8th: 6 doubles).
 template <int ORDER>
 __device__ double correct_particle(double *r, const double *f, double dt, double etapow,
-                                   double dtlim)
+                                   double dtlim, double *aux = nullptr)
 {
     double h, hinv;
     half_step(dt, h, hinv);
@@ -69,6 +71,10 @@ __device__ double correct_particle(double *r, const double *f, double dt, double
         st3(r + 4, vel1);
         st3(r + 8, fa);
         st3(r + 11, fj);
+        if (aux) {
+            st3(aux + 0, snp);
+            st3(aux + 3, crk);
+        }
         const double s0 = norm2(fa), s1 = norm2(fj), s2 = norm2(snp), s3 = norm2(crk);
         const double u = __dadd_rn(sqrt(__dmul_rn(s0, s2)), s1);
         const double l = __dadd_rn(sqrt(__dmul_rn(s1, s3)), s2);
@@ -93,6 +99,10 @@ __device__ double correct_particle(double *r, const double *f, double dt, double
         st3(r + 11, fj);
         st3(r + 14, fs);
         st3(r + 17, crk);
+        if (aux) {
+            st3(aux + 0, d4a);
+            st3(aux + 3, d5a);
+        }
         const double s0 = norm2(fa), s1 = norm2(fj), s2 = norm2(fs);
         const double s3 = norm2(crk), s4 = norm2(d4a), s5 = norm2(d5a);
         const double u = __dadd_rn(sqrt(__dmul_rn(s0, s2)), s1);
@@ -126,6 +136,10 @@ __device__ double correct_particle(double *r, const double *f, double dt, double
         st3(r + 17, fc);
         st3(r + 20, d4a);
         st3(r + 23, d5a);
+        if (aux) {
+            st3(aux + 0, d6a);
+            st3(aux + 3, d7a);
+        }
         const double s0 = norm2(fa), s1 = norm2(fj), s2 = norm2(fs);
         const double s5 = norm2(d5a), s6 = norm2(d6a), s7 = norm2(d7a);
         const double u = __dadd_rn(sqrt(__dmul_rn(s0, s2)), s1);

@@ -761,6 +761,7 @@ int run_teams(hb_ens *e, double tend, long long max_block_steps)
         TeamLaunch L;
         L.jp = e->d_jp;
         L.dt = e->d_dt;
+        L.aux = nullptr;
         L.sys = e->d_tsys + g.first;
         L.st = e->d_cstate;
         L.next_sys = e->d_team_next;

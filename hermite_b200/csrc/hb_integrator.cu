@@ -425,7 +425,7 @@ force_items_big_kernel(ItemsArgs a)
 template <int ORDER>
 __global__ void correct_kernel(double *__restrict__ jp, double *__restrict__ dt,
                                const double *__restrict__ force, const int *__restrict__ ilist,
-                               Sched *s)
+                               Sched *s, double *__restrict__ aux)
 {
     pdl_enter();
     constexpr int R = Rec<ORDER>::words, F = Frc<ORDER>::words;
@@ -434,7 +434,7 @@ __global__ void correct_kernel(double *__restrict__ jp, double *__restrict__ dt,
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nact; k += gridDim.x * blockDim.x) {
         const int i = ilist[k];
         const double dtn = correct_particle<ORDER>(jp + (size_t)i * R, force + (size_t)k * F, dt[i],
-                                                   etapow, dtlim);
+                                                   etapow, dtlim, aux + (size_t)i * kAuxWords);
         if (!(dtn >= 0x1p-48)) s->error = 1;   // timestep underflow (or NaN)
         dt[i] = dtn;
     }
@@ -560,7 +560,7 @@ static cudaError_t launch_step(const IntegratorLaunch &L, cudaStream_t s)
     }
     if (e == cudaSuccess)
         e = launch_pdl(correct_kernel<ORDER>, std::max(1, std::min(nb, L.nsm * 4)), 256, 0, s, L.jp,
-                       L.dt, (const double *)L.force, (const int *)L.ilist, L.sched);
+                       L.dt, (const double *)L.force, (const int *)L.ilist, L.sched, L.aux);
     return e;
 }
 

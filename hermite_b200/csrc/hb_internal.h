@@ -55,9 +55,15 @@ struct Sched {
     IntStatus *status;               // mapped mirror for the host
 };
 
+// Per slot, the two higher derivatives kept for dumps (see correct_particle).
+constexpr int kAuxWords = 6;
+// Particle::recalc_dt on the host, from a record and its aux row (hb_dump.cu).
+double recalc_dt(int order, const double *rec, const double *aux, double eta, double dtmax);
+
 struct IntegratorLaunch {
     double *jp;          // records (the state)
     double *dt;          // per-slot timestep
+    double *aux;         // per-slot dump derivatives [kAuxWords]
     int *ilist;          // active slots
     Sched *sched;
     double *force, *partial;
@@ -96,6 +102,7 @@ struct TeamConfig {
 };
 struct TeamLaunch {
     double *jp, *dt;
+    double *aux;       // per-slot dump derivatives [kAuxWords], or null
     const TeamSys *sys;
     TeamState *st;     // indexed by TeamSys::id
     int *next_sys;     // work counter, zero at launch

@@ -327,7 +327,9 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
                             for (int k = 0; k < F; ++k) f[k] += part[(size_t)(src * KM + a) * F + k];
                         const int q = cand[a];
                         double *r = rec + (size_t)q * R;
-                        const double dtn = correct_particle<ORDER>(r, f, dts[q], L.etapow, dtlim);
+                        const double dtn = correct_particle<ORDER>(
+                            r, f, dts[q], L.etapow, dtlim,
+                            L.aux ? L.aux + (size_t)(S.off + lo + q) * kAuxWords : nullptr);
                         if (!(dtn >= 0x1p-48)) misc[1] = 1;   // timestep underflow (or NaN)
                         dts[q] = dtn;
                         tn[q] = dtn + r[7];
@@ -375,7 +377,9 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
                         }
                         const int q = cand[a];
                         double *r = rec + (size_t)q * R;
-                        const double dtn = correct_particle<ORDER>(r, f, dts[q], L.etapow, dtlim);
+                        const double dtn = correct_particle<ORDER>(
+                            r, f, dts[q], L.etapow, dtlim,
+                            L.aux ? L.aux + (size_t)(S.off + lo + q) * kAuxWords : nullptr);
                         if (!(dtn >= 0x1p-48)) misc[1] = 1;
                         dts[q] = dtn;
                         tn[q] = dtn + r[7];

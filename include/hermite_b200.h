@@ -46,8 +46,9 @@ enum hb_status {
     HB_ERR_NO_DEVICE = 5,      /* no CUDA device, or not an sm_100 device  */
     HB_ERR_STATE = 6,          /* call out of order (e.g. force before any
                                   predict_all)                            */
-    HB_ERR_TOO_LARGE = 7       /* a size exceeds a fixed capacity (see
+    HB_ERR_TOO_LARGE = 7,      /* a size exceeds a fixed capacity (see
                                   hb_force_predicted_noalloc)             */
+    HB_ERR_IO = 8              /* a file could not be written or parsed   */
 };
 
 enum hb_precision {
@@ -188,6 +189,38 @@ int hb_integrator_stats(const hb_ctx *ctx, long long *particle_steps, long long 
 int hb_energy(hb_ctx *ctx, double eps2, double *kinetic, double *potential);
 /* Copy count records (and, if dt_out, their timesteps) from the device. */
 int hb_get_records(hb_ctx *ctx, int addr0, int count, double *records_out, double *dt_out);
+
+/* ---- checkpoints -----------------------------------------------------------
+ * The reference's dump format (NbodySystem::dump / restore,
+ * SRC/nbodysystem.h:405-446; Particle::dump / restore, SRC/hermite{4,6,8}.h):
+ * a header (order, dumpid, nbody, tsys, initial and previous energy, particle
+ * and block steps) and per particle id, mass, pos, vel, acc, jrk, snp, crk
+ * [d4a d5a [d6a d7a]] in %A hex floats.  Files written here restore in the
+ * reference's integrator and the reverse.
+ *
+ * Host-only helpers.  records: nbody j-particle records (tlast is not in a
+ * dump; the reader sets it to tsys); aux: nbody x 6 doubles, the two vectors
+ * beyond the record (snp crk at 4th order, d4a d5a at 6th, d6a d7a at 8th);
+ * ids: nbody ids (null on write: the slot index; null on read: dropped). */
+int hb_dump_write(const char *path, int order, int dumpid, int nbody, double tsys,
+                  double init_energy, double prev_energy, long long steps, long long block_steps,
+                  const long long *ids, const double *records, const double *aux);
+int hb_dump_read_header(const char *path, int *order, int *dumpid, int *nbody, double *tsys,
+                        double *init_energy, double *prev_energy, long long *steps,
+                        long long *block_steps);
+int hb_dump_read(const char *path, int order, int nbody, long long *ids, double *records,
+                 double *aux);
+/* Dump the device integrator's state.  Every particle must be at the block
+ * time (tsys a multiple of dtmax), as in the reference's dump intervals. */
+int hb_integrator_dump(hb_ctx *ctx, const char *path, int dumpid, double init_energy,
+                       double prev_energy);
+/* Restore a dump (order and N must match the context) and prepare the
+ * integrator as the reference's restore + reinitialize_steps do
+ * (SRC/nbodysystem.h:429-458): tlast = tsys for all, dt from recalc_dt(eta,
+ * dtmax); the dumped forces are the corrector's previous forces, no force
+ * evaluation.  Returns the dump id and the two energies. */
+int hb_integrator_restore(hb_ctx *ctx, const char *path, double eps2, double eta, double dtmax,
+                          int *dumpid, double *init_energy, double *prev_energy);
 
 /* ---- batched ensembles ---------------------------------------------------
  * No reference counterpart (the reference integrates one system per
