@@ -51,7 +51,8 @@ EXPORTED_SYMBOLS = (
     "hb_ens_set_cluster", "hb_ens_get_cluster", "hb_ens_cluster_offset", "hb_ens_init",
     "hb_ens_run", "hb_ens_stats", "hb_ens_energy", "hb_ens_set_engine", "hb_ens_cluster_engine",
     "hb_ens_cluster_stats", "hb_dump_write", "hb_dump_read_header", "hb_dump_read",
-    "hb_integrator_dump", "hb_integrator_restore",
+    "hb_integrator_dump", "hb_integrator_restore", "hb_snapshot_read_header", "hb_snapshot_read",
+    "hb_snapshot_write",
 )
 
 
@@ -188,6 +189,11 @@ def load_library() -> ctypes.CDLL:
                                     ctypes.POINTER(ctypes.c_longlong)]),
         "hb_dump_read": (I, [ctypes.c_char_p, I, I, ctypes.POINTER(ctypes.c_longlong), dp, dp]),
         "hb_integrator_dump": (I, [P, ctypes.c_char_p, I, D, D]),
+        "hb_snapshot_read_header": (I, [ctypes.c_char_p, ctypes.POINTER(I), ctypes.POINTER(I), dp]),
+        "hb_snapshot_read": (I, [ctypes.c_char_p, I, ctypes.POINTER(ctypes.c_longlong), dp, dp, dp,
+                                 dp]),
+        "hb_snapshot_write": (I, [ctypes.c_char_p, I, I, D, ctypes.POINTER(ctypes.c_longlong), dp,
+                                  dp, dp, dp]),
         "hb_integrator_restore": (I, [P, ctypes.c_char_p, D, D, D, ctypes.POINTER(I), dp, dp]),
     }
     for name, (res, args) in sig.items():

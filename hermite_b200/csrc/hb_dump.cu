@@ -1,4 +1,5 @@
-// hb_dump.cu -- checkpoints in the reference's dump format (host only).
+// hb_dump.cu -- checkpoints and snapshots in the reference's file formats
+// (host only).
 //
 // File layout (NbodySystem::dump / restore, SRC/nbodysystem.h:405-446):
 //   "%d %d\n%ld\n%20.16f\n"   order, dumpid, nbody, tsys
@@ -13,8 +14,12 @@
 // tlast acc jrk [snp crk [d4a d5a]]; the two higher vectors the corrector
 // derives on top of them (snp crk at 4th order, d4a d5a at 6th, d6a d7a at
 // 8th) travel in a separate 6-double "aux" row per particle.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <vector>
 
 #include "hermite_b200.h"
 #include "hb_internal.h"
@@ -147,6 +152,153 @@ int hb_dump_read(const char *path, int order, int nbody, long long *ids, double 
     }
     std::fclose(fp);
     return ok ? HB_OK : HB_ERR_IO;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Snapshots in the reference's text format (NbodySystem::read_snapshot_masaki
+// and write_snapshot_masaki, SRC/nbodysystem.h:359-403): "%d\n%ld\n%f\n"
+// (snapid, nbody, time), then per particle "%6ld    %A    %A %A %A    %A %A %A
+// %A" (id, mass, pos, vel, potential).  Large files are the start-up cost of
+// big runs, so both directions work on the whole file in memory and split the
+// particle lines over host threads.
+
+namespace {
+
+bool slurp(const char *path, std::string &buf)
+{
+    FILE *fp = std::fopen(path, "rb");
+    if (!fp) return false;
+    std::fseek(fp, 0, SEEK_END);
+    const long sz = std::ftell(fp);
+    std::fseek(fp, 0, SEEK_SET);
+    if (sz < 0) {
+        std::fclose(fp);
+        return false;
+    }
+    buf.resize((size_t)sz);
+    const size_t got = sz ? std::fread(&buf[0], 1, (size_t)sz, fp) : 0;
+    std::fclose(fp);
+    return got == (size_t)sz;
+}
+
+// Position after the header's three tokens; -1 if malformed.
+long parse_snap_header(const std::string &buf, int *snapid, long *n, double *t)
+{
+    const char *p = buf.c_str();
+    char *e = nullptr;
+    const long sid = std::strtol(p, &e, 10);
+    if (e == p) return -1;
+    p = e;
+    const long nb = std::strtol(p, &e, 10);
+    if (e == p || nb < 0) return -1;
+    p = e;
+    const double tt = std::strtod(p, &e);
+    if (e == p) return -1;
+    *snapid = (int)sid;
+    *n = nb;
+    *t = tt;
+    return (long)(e - buf.c_str());
+}
+
+}  // namespace
+
+extern "C" {
+
+int hb_snapshot_read_header(const char *path, int *snapid, int *nbody, double *tsys)
+{
+    if (!path) return HB_ERR_INVALID;
+    FILE *fp = std::fopen(path, "r");
+    if (!fp) return HB_ERR_IO;
+    int sid = 0;
+    long n = 0;
+    double t = 0.0;
+    const bool ok = std::fscanf(fp, "%d %ld %lf", &sid, &n, &t) == 3;
+    std::fclose(fp);
+    if (!ok || n < 0 || n > (1L << 30)) return HB_ERR_IO;
+    if (snapid) *snapid = sid;
+    if (nbody) *nbody = (int)n;
+    if (tsys) *tsys = t;
+    return HB_OK;
+}
+
+int hb_snapshot_read(const char *path, int nbody, long long *ids, double *mass, double *pos,
+                     double *vel, double *pot)
+{
+    if (!path || nbody < 0 || (nbody > 0 && (!mass || !pos || !vel))) return HB_ERR_INVALID;
+    std::string buf;
+    if (!slurp(path, buf)) return HB_ERR_IO;
+    int sid;
+    long n;
+    double t;
+    const long body = parse_snap_header(buf, &sid, &n, &t);
+    if (body < 0 || n != nbody) return HB_ERR_IO;
+    // line starts of the particle records
+    std::vector<long> start;
+    start.reserve((size_t)nbody + 1);
+    long p = body;
+    const long len = (long)buf.size();
+    while (p < len && (int)start.size() < nbody) {
+        while (p < len && (buf[p] == '\n' || buf[p] == '\r' || buf[p] == ' ' || buf[p] == '\t')) ++p;
+        if (p >= len) break;
+        start.push_back(p);
+        while (p < len && buf[p] != '\n') ++p;
+    }
+    if ((int)start.size() != nbody) return HB_ERR_IO;
+    int bad = 0;
+    const char *base = buf.c_str();
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (int i = 0; i < nbody; ++i) {
+        const char *q = base + start[i];
+        char *e = nullptr;
+        const long long id = std::strtoll(q, &e, 10);
+        bad |= e == q;
+        q = e;
+        double v[8];
+        for (int k = 0; k < 8; ++k) {
+            v[k] = std::strtod(q, &e);
+            bad |= e == q;
+            q = e;
+        }
+        if (ids) ids[i] = id;
+        mass[i] = v[0];
+        for (int k = 0; k < 3; ++k) {
+            pos[3 * (size_t)i + k] = v[1 + k];
+            vel[3 * (size_t)i + k] = v[4 + k];
+        }
+        if (pot) pot[i] = v[7];
+    }
+    return bad ? HB_ERR_IO : HB_OK;
+}
+
+int hb_snapshot_write(const char *path, int snapid, int nbody, double tsys, const long long *ids,
+                      const double *mass, const double *pos, const double *vel, const double *pot)
+{
+    if (!path || nbody < 0 || (nbody > 0 && (!mass || !pos || !vel))) return HB_ERR_INVALID;
+    FILE *fp = std::fopen(path, "w");
+    if (!fp) return HB_ERR_IO;
+    std::fprintf(fp, "%d\n%ld\n%f\n", snapid, (long)nbody, tsys);
+    constexpr int kBlock = 4096;   // particles formatted per task
+    const int nblk = (nbody + kBlock - 1) / kBlock;
+    std::vector<std::string> out((size_t)nblk);
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < nblk; ++b) {
+        std::string &s = out[b];
+        char line[512];
+        const int i1 = std::min(nbody, (b + 1) * kBlock);
+        for (int i = b * kBlock; i < i1; ++i) {
+            const double *x = pos + 3 * (size_t)i, *v = vel + 3 * (size_t)i;
+            const int m = std::snprintf(line, sizeof line, "%6ld    %A    %A %A %A    %A %A %A    %A\n",
+                                        (long)(ids ? ids[i] : i), mass[i], x[0], x[1], x[2], v[0],
+                                        v[1], v[2], pot ? pot[i] : 0.0);
+            s.append(line, (size_t)m);
+        }
+    }
+    bool ok = true;
+    for (const std::string &s : out) ok = ok && std::fwrite(s.data(), 1, s.size(), fp) == s.size();
+    ok = ok && !std::ferror(fp);
+    return (std::fclose(fp) == 0 && ok) ? HB_OK : HB_ERR_IO;
 }
 
 }  // extern "C"

@@ -10,7 +10,10 @@
   optional exact rescale to E = -1/4 with virial ratio 1/2.
 * `write_snapshot` / `read_snapshot` -- the hex-float text format read by
   NbodySystem::read_snapshot_masaki (SRC/nbodysystem.h:379-403) and written by
-  write_snapshot_masaki (:359-378) and gen-plum (RUN/gen-plum.c:240-252).
+  write_snapshot_masaki (:359-378) and gen-plum (RUN/gen-plum.c:240-252),
+  through the library's multi-threaded reader and writer
+  (hb_snapshot_read / hb_snapshot_write).  `read_snapshot_py` and
+  `write_snapshot_py` are plain-Python equivalents (no library needed).
 """
 from __future__ import annotations
 
@@ -120,7 +123,7 @@ def _hexf(x: float) -> str:
                                                              ("INF" if x > 0 else "-INF"))
 
 
-def write_snapshot(path, snap: Snapshot) -> None:
+def write_snapshot_py(path, snap: Snapshot) -> None:
     with open(path, "w") as fp:
         fp.write(f"{snap.snapid}\n{snap.n}\n{snap.t:f}\n")
         for i in range(snap.n):
@@ -137,7 +140,7 @@ def _parse(tok: str) -> float:
     return float(t)
 
 
-def read_snapshot(path) -> Snapshot:
+def read_snapshot_py(path) -> Snapshot:
     with open(path) as fp:
         toks = fp.read().split()
     snapid, n, t = int(toks[0]), int(toks[1]), float(toks[2])
@@ -147,6 +150,47 @@ def read_snapshot(path) -> Snapshot:
     a = np.array([_parse(s) for s in body], dtype=np.float64).reshape(n, 9)
     return Snapshot(snapid, t, a[:, 0].astype(np.int64), a[:, 1].copy(), a[:, 2:5].copy(),
                     a[:, 5:8].copy(), a[:, 8].copy())
+
+
+def _dp(a):
+    import ctypes
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def write_snapshot(path, snap: Snapshot) -> None:
+    import ctypes
+    import hermite_b200 as hb
+    lib = hb.load_library()
+    ids = np.ascontiguousarray(snap.ids, dtype=np.int64)
+    mass = np.ascontiguousarray(snap.mass, dtype=np.float64)
+    pos = np.ascontiguousarray(snap.pos, dtype=np.float64)
+    vel = np.ascontiguousarray(snap.vel, dtype=np.float64)
+    pot = np.ascontiguousarray(snap.pot, dtype=np.float64)
+    st = lib.hb_snapshot_write(str(path).encode(), int(snap.snapid), snap.n, float(snap.t),
+                               ids.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), _dp(mass),
+                               _dp(pos), _dp(vel), _dp(pot))
+    if st != 0:
+        raise hb.HermiteError(st, f"hb_snapshot_write {path}")
+
+
+def read_snapshot(path) -> Snapshot:
+    import ctypes
+    import hermite_b200 as hb
+    lib = hb.load_library()
+    sid, n, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    st = lib.hb_snapshot_read_header(str(path).encode(), ctypes.byref(sid), ctypes.byref(n),
+                                     ctypes.byref(t))
+    if st != 0:
+        raise hb.HermiteError(st, f"hb_snapshot_read_header {path}")
+    ids = np.empty(n.value, dtype=np.int64)
+    mass, pot = np.empty(n.value), np.empty(n.value)
+    pos, vel = np.empty((n.value, 3)), np.empty((n.value, 3))
+    st = lib.hb_snapshot_read(str(path).encode(), n.value,
+                              ids.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), _dp(mass),
+                              _dp(pos), _dp(vel), _dp(pot))
+    if st != 0:
+        raise hb.HermiteError(st, f"hb_snapshot_read {path}")
+    return Snapshot(sid.value, t.value, ids, mass, pos, vel, pot)
 
 
 def records(snap: Snapshot, order: int, tlast: float = 0.0,

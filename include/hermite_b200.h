@@ -222,6 +222,19 @@ int hb_integrator_dump(hb_ctx *ctx, const char *path, int dumpid, double init_en
 int hb_integrator_restore(hb_ctx *ctx, const char *path, double eps2, double eta, double dtmax,
                           int *dumpid, double *init_energy, double *prev_energy);
 
+/* ---- snapshots -------------------------------------------------------------
+ * The reference's snapshot text format (read_snapshot_masaki /
+ * write_snapshot_masaki, SRC/nbodysystem.h:359-403): "%d\n%ld\n%f\n" (snapid,
+ * nbody, time), then per particle id, mass, pos[3], vel[3], potential as
+ * "%6ld    %A    %A %A %A    %A %A %A    %A".  Host only; the particle lines
+ * are parsed and formatted on several host threads.  pos / vel: nbody x 3;
+ * ids and pot may be null (write: slot index / 0). */
+int hb_snapshot_read_header(const char *path, int *snapid, int *nbody, double *tsys);
+int hb_snapshot_read(const char *path, int nbody, long long *ids, double *mass, double *pos,
+                     double *vel, double *pot);
+int hb_snapshot_write(const char *path, int snapid, int nbody, double tsys, const long long *ids,
+                      const double *mass, const double *pos, const double *vel, const double *pot);
+
 /* ---- batched ensembles ---------------------------------------------------
  * No reference counterpart (the reference integrates one system per
  * process).  Many independent clusters (any sizes, softenings, masses)
