@@ -16,10 +16,12 @@
 #include "hb_internal.h"
 
 namespace hb {
+// compiled launch shapes per order and precision (hb_force_table.cuh)
+constexpr int kNumVariants = 20;
 const ForceVariant *force_variant_64(int order, int v);
 const ForceVariant *force_variant_mixed(int order, int v);
 
-int force_variant_count(int order, bool) { return (order == 4 || order == 6 || order == 8) ? 18 : 0; }
+int force_variant_count(int order, bool) { return (order == 4 || order == 6 || order == 8) ? kNumVariants : 0; }
 
 const ForceVariant *force_variant(int order, bool mixed, int v)
 {
@@ -35,7 +37,6 @@ constexpr int kMaxBody = 1 << 24;
 constexpr size_t kEagerUploadBytes = (size_t)4 << 20, kUploadChunkBytes = (size_t)2 << 20;
 // HB_ENGINE_AUTO takes the team engine up to this many particles.
 constexpr int kTeamAutoMaxBody = 3072;
-constexpr int kNumVariants = 20;
 
 int rec_words(int order) { return 8 + 3 * (order - 2); }
 int force_words(int order) { return 3 * (order / 2); }

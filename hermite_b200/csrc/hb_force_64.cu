@@ -8,6 +8,7 @@ const ForceVariant *force_variant_64(int order, int v)
     static const VariantTable<4, false> t4;
     static const VariantTable<6, false> t6;
     static const VariantTable<8, false> t8;
+    static_assert(VariantTable<4, false>::count == 20, "keep kNumVariants in hb_capi.cu in step");
     if (v < 0 || v >= VariantTable<4, false>::count) return nullptr;
     switch (order) {
     case 4: return &t4.v[v];
