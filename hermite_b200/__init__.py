@@ -31,7 +31,8 @@ __all__ = ["Gravity", "Ensemble", "HermiteError", "record_words", "force_words",
 
 FP64 = 0
 MIXED = 1
-_PREC = {"fp64": FP64, "mixed": MIXED, FP64: FP64, MIXED: MIXED}
+FP64_DD = 2      # 8th order with double-double positions (records: 29 words)
+_PREC = {"fp64": FP64, "mixed": MIXED, "dd": FP64_DD, FP64: FP64, MIXED: MIXED, FP64_DD: FP64_DD}
 
 _PKG = Path(__file__).resolve().parent
 _LIB_PATH = _PKG / "_lib" / "libhermite_b200.so"
@@ -87,9 +88,11 @@ def write_dump(path, order: int, records, aux, tsys: float, dumpid: int = 0,
         raise HermiteError(st, f"hb_dump_write {path}: " + lib.hb_status_string(st).decode())
 
 
-def read_dump(path) -> dict:
+def read_dump(path, dd: bool = False) -> dict:
     """Read a checkpoint in the reference's dump format (host only): header
-    fields, ids, records (tlast = tsys) and the aux derivatives."""
+    fields, ids, records (tlast = tsys) and the aux derivatives.  dd: the file
+    holds double-double positions (the header says order 8 for both), read
+    into 29-word records with order code 9."""
     lib = load_library()
     o, d, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     t, e0, e1 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
@@ -99,14 +102,15 @@ def read_dump(path) -> dict:
                                  ctypes.byref(e1), ctypes.byref(ps), ctypes.byref(bs))
     if st != 0:
         raise HermiteError(st, f"hb_dump_read_header {path}: " + lib.hb_status_string(st).decode())
-    rec = np.empty((n.value, record_words(o.value)))
+    code = 9 if dd else o.value
+    rec = np.empty((n.value, record_words(code)))
     aux = np.empty((n.value, AUX_WORDS))
     ids = np.empty(n.value, dtype=np.int64)
-    st = lib.hb_dump_read(str(path).encode(), o.value, n.value,
+    st = lib.hb_dump_read(str(path).encode(), code, n.value,
                           ids.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), _dptr(rec), _dptr(aux))
     if st != 0:
         raise HermiteError(st, f"hb_dump_read {path}: " + lib.hb_status_string(st).decode())
-    return {"order": o.value, "dumpid": d.value, "nbody": n.value, "tsys": t.value,
+    return {"order": code, "dumpid": d.value, "nbody": n.value, "tsys": t.value,
             "energies": (e0.value, e1.value), "steps": (ps.value, bs.value), "ids": ids,
             "records": rec, "aux": aux}
 
@@ -221,9 +225,12 @@ class Gravity:
     """The reference's `struct Gravity`, one CUDA context-owned instance."""
 
     def __init__(self, order: int, nbody: int, precision="fp64"):
+        """precision: "fp64", "mixed", or "dd" (order 8 only: double-double
+        positions; records carry posL after the 8th-order fields, 29 words)."""
         self._lib = load_library()
         self.order, self.nbody = int(order), int(nbody)
-        self.R, self.F = record_words(self.order), force_words(self.order)
+        self.dd = _PREC[precision] == FP64_DD
+        self.R, self.F = record_words(9 if self.dd else self.order), force_words(self.order)
         h = ctypes.c_void_p()
         st = self._lib.hb_create(self.order, self.nbody, _PREC[precision], ctypes.byref(h))
         if st != 0:
@@ -263,8 +270,8 @@ class Gravity:
         pos = np.ascontiguousarray(pos, dtype=np.float64)
         vel = np.ascontiguousarray(vel, dtype=np.float64)
         derivs = np.ascontiguousarray(derivs, dtype=np.float64).reshape(-1)
-        if derivs.size != 3 * (self.order - 2):
-            raise ValueError(f"derivs needs {3 * (self.order - 2)} values")
+        if derivs.size != self.R - 8:
+            raise ValueError(f"derivs needs {self.R - 8} values")
         self._check(self._lib.hb_set_jp(self._h, int(addr), _dptr(pos), float(mass), _dptr(vel),
                                         float(tlast), _dptr(derivs)), "set_jp")
 

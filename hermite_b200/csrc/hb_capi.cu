@@ -21,7 +21,10 @@ constexpr int kNumVariants = 20;
 const ForceVariant *force_variant_64(int order, int v);
 const ForceVariant *force_variant_mixed(int order, int v);
 
-int force_variant_count(int order, bool) { return (order == 4 || order == 6 || order == 8) ? kNumVariants : 0; }
+int force_variant_count(int order, bool mixed)
+{
+    return (order == 4 || order == 6 || order == 8 || (order == 9 && !mixed)) ? kNumVariants : 0;
+}
 
 const ForceVariant *force_variant(int order, bool mixed, int v)
 {
@@ -40,7 +43,7 @@ constexpr int kTeamAutoMaxBody = 3072;
 
 int rec_words(int order) { return 8 + 3 * (order - 2); }
 int force_words(int order) { return 3 * (order / 2); }
-int pred64_ncomp(int order) { return 7 + 3 * (order / 2 - 2); }
+int pred64_ncomp(int order) { return 7 + 3 * (order / 2 - 2) + (order == 9 ? 3 : 0); }
 int predmx_ncomp(int order) { return 10 + 3 * (order / 2 - 2); }
 }  // namespace
 
@@ -225,7 +228,8 @@ int pick_variant(const hb_ctx *c, int nact, int *jsplit_hint)
     *jsplit_hint = 0;
     if (c->variant_override >= 0) return c->variant_override;
     const bool mixed = c->pred_precision == HB_MIXED;
-    if (const TuneEntry *e = lookup_tuning(c->order, mixed, c->nbody, nact)) {
+    // double-double (order 9) uses the 8th-order measurements
+    if (const TuneEntry *e = lookup_tuning(c->order == 9 ? 8 : c->order, mixed, c->nbody, nact)) {
         const ForceVariant *fv = force_variant(c->order, mixed, e->variant);
         if (fv) {
             const long long gx_bucket = ((1LL << e->log2nact) + fv->ti - 1) / fv->ti;
@@ -370,9 +374,15 @@ int hb_create(int order, int nbody, int precision, hb_ctx **out)
 {
     if (!out) return HB_ERR_INVALID;
     *out = nullptr;
+    // HB_FP64_DD: 8th order with double-double positions, internal order 9
+    const bool dd = precision == HB_FP64_DD;
     if (!valid_order(order) || nbody < 1 || nbody > kMaxBody ||
-        (precision != HB_FP64 && precision != HB_MIXED))
+        (precision != HB_FP64 && precision != HB_MIXED && !(dd && order == 8)))
         return HB_ERR_INVALID;
+    if (dd) {
+        order = 9;
+        precision = HB_FP64;
+    }
 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return HB_ERR_NO_DEVICE;
@@ -406,7 +416,7 @@ int hb_create(int order, int nbody, int precision, hb_ctx **out)
     ok = ok && cudaMalloc((void **)&ctx->d_jp, np * ctx->R * sizeof(double)) == cudaSuccess;
     ok = ok && cudaMalloc((void **)&ctx->d_force, np * ctx->F * sizeof(double)) == cudaSuccess;
     ok = ok && cudaMalloc((void **)&ctx->d_pot, np * sizeof(double)) == cudaSuccess;
-    ok = ok && cudaMalloc((void **)&ctx->d_posm, np * 4 * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc((void **)&ctx->d_posm, np * (order == 9 ? 7 : 4) * sizeof(double)) == cudaSuccess;
     ok = ok && cudaMalloc((void **)&ctx->d_partial, ctx->partial_cap * sizeof(double)) == cudaSuccess;
     ok = ok && cudaMalloc(&ctx->d_pred, pred_bytes) == cudaSuccess;
     ok = ok && cudaMalloc((void **)&ctx->d_counter, (np / 32 + 1) * sizeof(unsigned)) == cudaSuccess;
@@ -576,13 +586,21 @@ int hb_potential(hb_ctx *ctx, double eps2, double *pot_out)
 int hb_set_precision(hb_ctx *ctx, int precision)
 {
     if (!ctx) return HB_ERR_INVALID;
+    if (ctx->order == 9) {
+        if (precision != HB_FP64_DD && precision != HB_FP64)
+            return fail(ctx, HB_ERR_INVALID, "a double-double context stays double-double");
+        return HB_OK;
+    }
     if (precision != HB_FP64 && precision != HB_MIXED)
         return fail(ctx, HB_ERR_INVALID, "precision %d unknown", precision);
     ctx->precision = precision;
     return HB_OK;
 }
 
-int hb_get_precision(const hb_ctx *ctx) { return ctx ? ctx->precision : -1; }
+int hb_get_precision(const hb_ctx *ctx)
+{
+    return ctx ? (ctx->order == 9 ? HB_FP64_DD : ctx->precision) : -1;
+}
 
 int hb_set_stream(hb_ctx *ctx, void *cuda_stream)
 {
@@ -615,14 +633,22 @@ int hb_set_force_shape(hb_ctx *ctx, int variant, int jsplit)
 
 int hb_force_variant_count(int order, int precision)
 {
-    if (!valid_order(order) || (precision != HB_FP64 && precision != HB_MIXED)) return 0;
+    if (!valid_order(order)) return 0;
+    if (precision == HB_FP64_DD) return order == 8 ? force_variant_count(9, false) : 0;
+    if (precision != HB_FP64 && precision != HB_MIXED) return 0;
     return force_variant_count(order, precision == HB_MIXED);
 }
 
 int hb_force_variant_info(int order, int precision, int variant, int *threads, int *i_per_thread,
                           int *j_warps)
 {
-    if (!valid_order(order) || (precision != HB_FP64 && precision != HB_MIXED)) return HB_ERR_INVALID;
+    if (!valid_order(order)) return HB_ERR_INVALID;
+    if (precision == HB_FP64_DD) {
+        if (order != 8) return HB_ERR_INVALID;
+        order = 9;
+        precision = HB_FP64;
+    }
+    if (precision != HB_FP64 && precision != HB_MIXED) return HB_ERR_INVALID;
     const ForceVariant *fv = force_variant(order, precision == HB_MIXED, variant);
     if (!fv) return HB_ERR_INVALID;
     if (threads) *threads = fv->nw * 32;
@@ -673,7 +699,8 @@ int setup_integrator(hb_ctx *ctx, double tsys, double eps2, double eta, double d
     sc.tsys = tsys;
     sc.tend = tsys;
     sc.eps2 = eps2;
-    sc.etapow = std::pow(eta, 2.0 * (ctx->order - 3));   // set_run_params, SRC/nbodysystem.h:472
+    // set_run_params (SRC/nbodysystem.h:472); the double-double scheme is 8th order
+    sc.etapow = std::pow(eta, 2.0 * ((ctx->order == 9 ? 8 : ctx->order) - 3));
     sc.dtmax = dtmax;
     sc.particle_steps = particle_steps;
     sc.block_steps = block_steps;
@@ -810,20 +837,20 @@ int hb_integrator_restore(hb_ctx *ctx, const char *path, double eps2, double eta
     long long steps = 0, bsteps = 0;
     int s = hb_dump_read_header(path, &order, &did, &nb, &tsys, &e0, &e1, &steps, &bsteps);
     if (s != HB_OK) return fail(ctx, s, "cannot read the dump header of %s", path);
-    if (order != ctx->order || nb != ctx->nbody)
+    if (order != (ctx->order == 9 ? 8 : ctx->order) || nb != ctx->nbody)
         return fail(ctx, HB_ERR_INVALID, "the dump holds order %d, N = %d; the context order %d, N = %d",
                     order, nb, ctx->order, ctx->nbody);
     s = reset_integrator(ctx);
     if (s != HB_OK) return s;
     const size_t n = nb;
     std::vector<double> rec(n * ctx->R), aux(n * kAuxWords), dt(n);
-    s = hb_dump_read(path, order, nb, nullptr, rec.data(), aux.data());
+    s = hb_dump_read(path, ctx->order, nb, nullptr, rec.data(), aux.data());
     if (s != HB_OK) return fail(ctx, s, "cannot read the dump particles of %s", path);
     // NbodySystem::restore + reinitialize_steps (SRC/nbodysystem.h:429-458):
     // tlast = tsys, dt from recalc_dt
     for (size_t i = 0; i < n; ++i) {
         rec[i * ctx->R + 7] = tsys;
-        dt[i] = recalc_dt(order, rec.data() + i * ctx->R, aux.data() + i * kAuxWords, eta, dtmax);
+        dt[i] = recalc_dt(ctx->order, rec.data() + i * ctx->R, aux.data() + i * kAuxWords, eta, dtmax);
     }
     wait_upload(ctx);
     std::memcpy(ctx->h_jp, rec.data(), rec.size() * sizeof(double));

@@ -10,14 +10,23 @@ namespace hb {
 //
 // j-particle record (host mirror and its device copy), AoS doubles:
 //   pos[3] mass vel[3] tlast acc[3] jrk[3] [snp crk] [d4a d5a]
+//
+// ORDER 9 is the 8th-order scheme with double-double positions (the
+// reference's SRC/hermite8dd.h): the 8th-order record followed by the low
+// part of the position, posL[3] -- 29 words.  Its predicted state is the
+// 8th-order one (with the high part posH as the position) followed by the
+// predicted low part xL[3]; its force record is the 8th-order one.
 template <int ORDER> struct Rec {
-    static constexpr int words = 8 + 3 * (ORDER - 2);   // 14 / 20 / 26
-    static constexpr int bytes = words * 8;               // 112 / 160 / 208
+    static constexpr int words = 8 + 3 * (ORDER - 2);   // 14 / 20 / 26 / 29
+    static constexpr int bytes = words * 8;               // 112 / 160 / 208 / 232
 };
 // force record: acc jrk [snp] [crk]
 template <int ORDER> struct Frc {
-    static constexpr int words = 3 * (ORDER / 2);       // 6 / 9 / 12
+    static constexpr int words = 3 * (ORDER / 2);       // 6 / 9 / 12 / 12
 };
+// Offset of posL in an ORDER 9 record.
+constexpr int kRecPosL = 26;
+
 
 // Predicted j-particles: "AoSoA32" -- chunks of 32 slots, each chunk holding
 // one 32-wide vector per component, so that a warp's per-component loads and
@@ -28,7 +37,7 @@ template <int ORDER> struct Frc {
 //                                                                   10/13/16
 constexpr int kChunk = 32;
 template <int ORDER> struct Pred64 {
-    static constexpr int ncomp = 7 + 3 * (ORDER / 2 - 2);
+    static constexpr int ncomp = 7 + 3 * (ORDER / 2 - 2) + (ORDER == 9 ? 3 : 0);   // 7/10/13/16
     static constexpr int chunk_bytes = ncomp * kChunk * 8;
 };
 template <int ORDER> struct PredMx {
@@ -36,7 +45,7 @@ template <int ORDER> struct PredMx {
     static constexpr int chunk_bytes = ncomp * kChunk * 4;
 };
 // Component indices.
-enum : int { P64_X = 0, P64_M = 3, P64_V = 4, P64_A = 7, P64_J = 10 };
+enum : int { P64_X = 0, P64_M = 3, P64_V = 4, P64_A = 7, P64_J = 10, P64_XL = 13 };
 enum : int { PMX_XH = 0, PMX_XL = 3, PMX_M = 6, PMX_V = 7, PMX_A = 10, PMX_J = 13 };
 
 // Slots are padded to a multiple of this (i-tiles never read past the end).

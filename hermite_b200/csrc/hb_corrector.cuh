@@ -46,7 +46,9 @@ __device__ __forceinline__ double norm2(V3 a)
 }
 
 // Particle state in a j-particle record r (pos mass vel tlast acc jrk [snp
-// crk] [d4a d5a]); f = the new force (acc jrk [snp] [crk]).  Returns the new
+// crk] [d4a d5a] [posL]); f = the new force (acc jrk [snp] [crk]).  ORDER 9
+// is the 8th-order corrector with double-double positions
+// (Particle::correct, SRC/hermite8dd.h:187-239).  Returns the new
 // dt; writes the corrected state into r.  If aux is not null it receives the
 // two higher derivatives the reference's Particle also keeps and dumps (snp
 // crk at 4th order, d4a d5a at 6th, d6a d7a at 8th: 6 doubles).
@@ -115,7 +117,7 @@ __device__ double correct_particle(double *r, const double *f, double dt, double
         const V3 Sp = (fs + snp) * hh, Sm = (fs - snp) * hh;
         const V3 Cp = (fc + crk0) * hhh, Cm = (fc - crk0) * hhh;
         const V3 vel1 = vel + h * (((Ap + (-3. / 7.) * Jm) + (2. / 21) * Sp) - (1. / 105.) * Cm);
-        const V3 pos1 = pos + h * ((vel + vel1) + h * (((-3. / 7.) * Am + (2. / 21) * Jp) - (1. / 105.) * Sm));
+        const V3 dpos = h * ((vel + vel1) + h * (((-3. / 7.) * Am + (2. / 21) * Jp) - (1. / 105.) * Sm));
         const double hinv2 = __dmul_rn(hinv, hinv), hinv3 = __dmul_rn(hinv2, hinv);
         const double hinv4 = __dmul_rn(hinv2, hinv2), hinv5 = __dmul_rn(hinv2, hinv3);
         const double hinv6 = __dmul_rn(hinv3, hinv3), hinv7 = __dmul_rn(hinv3, hinv4);
@@ -128,7 +130,24 @@ __device__ double correct_particle(double *r, const double *f, double dt, double
         d4a = d4a + h * (d5a + h2 * (d6a + h3 * d7a));
         d5a = d5a + h * (d6a + h2 * d7a);
         d6a = d6a + h * d7a;
-        st3(r + 0, pos1);
+        if constexpr (ORDER == 9) {
+            // double-double position: dd_accumulate(posH, posL, dpos)
+            // (SRC/hermite8dd.h:4-23,203)
+            double *xh = r, *xl = r + kRecPosL;
+            const double dp[3] = {dpos.x, dpos.y, dpos.z};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double yh = __dadd_rn(xh[k], dp[k]);
+                const double res = __dsub_rn(dp[k], __dsub_rn(yh, xh[k]));
+                const double yl = __dadd_rn(xl[k], res);
+                const double zh = __dadd_rn(yh, yl);
+                const double zl = __dsub_rn(yl, __dsub_rn(zh, yh));
+                xh[k] = zh;
+                xl[k] = zl;
+            }
+        } else {
+            st3(r + 0, pos + dpos);
+        }
         st3(r + 4, vel1);
         st3(r + 8, fa);
         st3(r + 11, fj);

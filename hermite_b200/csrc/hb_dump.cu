@@ -9,6 +9,9 @@
 //   SRC/hermite6.h:49-60, SRC/hermite8.h:61-74):
 //   "%8ld %A" id, mass, then "   %A %A %A" for pos vel acc jrk snp crk
 //   [d4a d5a [d6a d7a]] -- order + 2 vectors.
+// Order code 9 is the 8th order with double-double positions
+// (SRC/hermite8dd.h:79-114): the header says order 8 and the low part of the
+// position follows the high part (posH posL vel acc ... d7a, 11 vectors).
 // tlast is not stored: a dump is taken when every particle is at tsys, and
 // the restore sets tlast = tsys.  Our j-particle records hold pos mass vel
 // tlast acc jrk [snp crk [d4a d5a]]; the two higher vectors the corrector
@@ -22,6 +25,7 @@
 #include <vector>
 
 #include "hermite_b200.h"
+#include "hb_common.cuh"
 #include "hb_internal.h"
 
 namespace hb {
@@ -73,21 +77,24 @@ int hb_dump_write(const char *path, int order, int dumpid, int nbody, double tsy
                   double init_energy, double prev_energy, long long steps, long long block_steps,
                   const long long *ids, const double *records, const double *aux)
 {
-    if (!path || (order != 4 && order != 6 && order != 8) || nbody < 0 ||
+    if (!path || (order != 4 && order != 6 && order != 8 && order != 9) || nbody < 0 ||
         (nbody > 0 && (!records || !aux)))
         return HB_ERR_INVALID;
     FILE *fp = std::fopen(path, "w");
     if (!fp) return HB_ERR_IO;
     const int R = 8 + 3 * (order - 2);
-    std::fprintf(fp, "%d %d\n%ld\n%20.16f\n", order, dumpid, (long)nbody, tsys);
+    const int Rd = order == 9 ? hb::kRecPosL : R;   // end of the derivative words
+    std::fprintf(fp, "%d %d\n%ld\n%20.16f\n", order == 9 ? 8 : order, dumpid, (long)nbody, tsys);
     std::fprintf(fp, "%A %A\n", init_energy, prev_energy);
     std::fprintf(fp, "%ld %ld\n", (long)steps, (long)block_steps);
     for (int i = 0; i < nbody; ++i) {
         const double *r = records + (size_t)i * R, *x = aux + (size_t)i * kAuxWords;
         std::fprintf(fp, "%8ld %A", (long)(ids ? ids[i] : i), r[3]);
         std::fprintf(fp, "   %A %A %A", r[0], r[1], r[2]);
+        if (order == 9)
+            std::fprintf(fp, "   %A %A %A", r[hb::kRecPosL], r[hb::kRecPosL + 1], r[hb::kRecPosL + 2]);
         std::fprintf(fp, "   %A %A %A", r[4], r[5], r[6]);
-        for (int k = 8; k < R; k += 3) std::fprintf(fp, "   %A %A %A", r[k], r[k + 1], r[k + 2]);
+        for (int k = 8; k < Rd; k += 3) std::fprintf(fp, "   %A %A %A", r[k], r[k + 1], r[k + 2]);
         std::fprintf(fp, "   %A %A %A", x[0], x[1], x[2]);
         std::fprintf(fp, "   %A %A %A", x[3], x[4], x[5]);
         std::fprintf(fp, "\n");
@@ -125,7 +132,7 @@ int hb_dump_read_header(const char *path, int *order, int *dumpid, int *nbody, d
 int hb_dump_read(const char *path, int order, int nbody, long long *ids, double *records,
                  double *aux)
 {
-    if (!path || (order != 4 && order != 6 && order != 8) || nbody < 0 ||
+    if (!path || (order != 4 && order != 6 && order != 8 && order != 9) || nbody < 0 ||
         (nbody > 0 && (!records || !aux)))
         return HB_ERR_INVALID;
     FILE *fp = std::fopen(path, "r");
@@ -135,16 +142,20 @@ int hb_dump_read(const char *path, int order, int nbody, long long *ids, double 
     double t = 0.0, e0 = 0.0, e1 = 0.0;
     bool ok = std::fscanf(fp, "%d %d %ld %lf", &o, &d, &n, &t) == 4 &&
               std::fscanf(fp, "%lA %lA", &e0, &e1) == 2 && std::fscanf(fp, "%ld %ld", &st, &bs) == 2 &&
-              o == order && n == nbody;
+              o == (order == 9 ? 8 : order) && n == nbody;
     const int R = 8 + 3 * (order - 2);
+    const int Rd = order == 9 ? hb::kRecPosL : R;
     for (int i = 0; ok && i < nbody; ++i) {
         double *r = records + (size_t)i * R, *x = aux + (size_t)i * kAuxWords;
         long id = 0;
         ok = std::fscanf(fp, "%ld %lA", &id, &r[3]) == 2 &&
-             std::fscanf(fp, "%lA %lA %lA", &r[0], &r[1], &r[2]) == 3 &&
-             std::fscanf(fp, "%lA %lA %lA", &r[4], &r[5], &r[6]) == 3;
+             std::fscanf(fp, "%lA %lA %lA", &r[0], &r[1], &r[2]) == 3;
+        if (ok && order == 9)
+            ok = std::fscanf(fp, "%lA %lA %lA", &r[hb::kRecPosL], &r[hb::kRecPosL + 1],
+                             &r[hb::kRecPosL + 2]) == 3;
+        ok = ok && std::fscanf(fp, "%lA %lA %lA", &r[4], &r[5], &r[6]) == 3;
         r[7] = t;
-        for (int k = 8; ok && k < R; k += 3)
+        for (int k = 8; ok && k < Rd; k += 3)
             ok = std::fscanf(fp, "%lA %lA %lA", &r[k], &r[k + 1], &r[k + 2]) == 3;
         ok = ok && std::fscanf(fp, "%lA %lA %lA", &x[0], &x[1], &x[2]) == 3 &&
              std::fscanf(fp, "%lA %lA %lA", &x[3], &x[4], &x[5]) == 3;

@@ -64,11 +64,11 @@ __device__ __noinline__ void predict_tile(const double *raw, int nslot, int slot
 {
     constexpr int R = Rec<ORDER>::words;
     for (int q = threadIdx.x; q < nslot; q += blockDim.x) {
-        double x[3], v[3], a[3] = {0, 0, 0}, jk[3] = {0, 0, 0}, m;
+        double x[3], v[3], a[3] = {0, 0, 0}, jk[3] = {0, 0, 0}, xl[3] = {0, 0, 0}, m;
         const int slot = slot0 + q;
         if (slot < n) {
             const double *r = raw + (size_t)q * R;
-            predict_slot<ORDER>(r, tsys, x, v, a, jk);
+            predict_slot<ORDER>(r, tsys, x, v, a, jk, xl);
             m = r[3];
         } else {
             for (int k = 0; k < 3; ++k) { x[k] = pad_position(slot, k); v[k] = 0.0; }
@@ -96,7 +96,8 @@ __device__ __noinline__ void predict_tile(const double *raw, int nslot, int slot
                 c[(P64_X + k) * 32] = x[k];
                 c[(P64_V + k) * 32] = v[k];
                 if constexpr (ORDER >= 6) c[(P64_A + k) * 32] = a[k];
-                if constexpr (ORDER == 8) c[(P64_J + k) * 32] = jk[k];
+                if constexpr (ORDER >= 8) c[(P64_J + k) * 32] = jk[k];
+                if constexpr (ORDER == 9) c[(P64_XL + k) * 32] = xl[k];
             }
             c[P64_M * 32] = m;
         }
@@ -116,9 +117,13 @@ __device__ __forceinline__ void load_i64(const double *pred, int ci, int lane, B
 #pragma unroll
         for (int k = 0; k < 3; ++k) b.a[k] = c[(P64_A + k) * 32];
     }
-    if constexpr (ORDER == 8) {
+    if constexpr (ORDER >= 8) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) b.jk[k] = c[(P64_J + k) * 32];
+    }
+    if constexpr (ORDER == 9) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) b.xl[k] = c[(P64_XL + k) * 32];
     }
 }
 
@@ -153,8 +158,11 @@ __device__ __forceinline__ void chunk64(const double *cp, const Body64 (&I)[NI],
             if constexpr (ORDER >= 6) {
                 w = *reinterpret_cast<const double2 *>(cp + (P64_A + k) * 32 + jl); J0.a[k] = w.x; J1.a[k] = w.y;
             }
-            if constexpr (ORDER == 8) {
+            if constexpr (ORDER >= 8) {
                 w = *reinterpret_cast<const double2 *>(cp + (P64_J + k) * 32 + jl); J0.jk[k] = w.x; J1.jk[k] = w.y;
+            }
+            if constexpr (ORDER == 9) {
+                w = *reinterpret_cast<const double2 *>(cp + (P64_XL + k) * 32 + jl); J0.xl[k] = w.x; J1.xl[k] = w.y;
             }
         }
         w = *reinterpret_cast<const double2 *>(cp + P64_M * 32 + jl); J0.m = w.x; J1.m = w.y;

@@ -544,19 +544,27 @@ static cudaError_t launch_step(const IntegratorLaunch &L, cudaStream_t s)
                 L.partial_cap, L.target_items, kBigNact};
     // both force shapes are in every step; the one not meant for this step's
     // nact (known on the device only) returns at once
-    if (e == cudaSuccess) {
-        if (L.mixed)
-            e = launch_pdl(force_items_kernel<ORDER, true>, L.items_grid, 128, L.smem_mixed, s, a);
-        else
+    if constexpr (ORDER == 9) {   // double-double positions: FP64 only
+        if (e == cudaSuccess)
             e = launch_pdl(force_items_kernel<ORDER, false>, L.items_grid, 128, L.smem_fp64, s, a);
-    }
-    if (e == cudaSuccess) {
-        if (L.mixed)
-            e = launch_pdl(force_items_big_kernel<ORDER, true>, L.big_grid, 128,
-                           BigShape<ORDER, true>::smem_bytes, s, a);
-        else
+        if (e == cudaSuccess)
             e = launch_pdl(force_items_big_kernel<ORDER, false>, L.big_grid, 128,
                            BigShape<ORDER, false>::smem_bytes, s, a);
+    } else {
+        if (e == cudaSuccess) {
+            if (L.mixed)
+                e = launch_pdl(force_items_kernel<ORDER, true>, L.items_grid, 128, L.smem_mixed, s, a);
+            else
+                e = launch_pdl(force_items_kernel<ORDER, false>, L.items_grid, 128, L.smem_fp64, s, a);
+        }
+        if (e == cudaSuccess) {
+            if (L.mixed)
+                e = launch_pdl(force_items_big_kernel<ORDER, true>, L.big_grid, 128,
+                               BigShape<ORDER, true>::smem_bytes, s, a);
+            else
+                e = launch_pdl(force_items_big_kernel<ORDER, false>, L.big_grid, 128,
+                               BigShape<ORDER, false>::smem_bytes, s, a);
+        }
     }
     if (e == cudaSuccess)
         e = launch_pdl(correct_kernel<ORDER>, std::max(1, std::min(nb, L.nsm * 4)), 256, 0, s, L.jp,
@@ -570,6 +578,7 @@ cudaError_t integrator_step_launch(int order, const IntegratorLaunch &L, cudaStr
     case 4: return launch_step<4>(L, s);
     case 6: return launch_step<6>(L, s);
     case 8: return launch_step<8>(L, s);
+    case 9: return launch_step<9>(L, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -589,6 +598,7 @@ cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *grid_
     case 13: HB_ITEMS(6, true) break;
     case 16: HB_ITEMS(8, false) break;
     case 17: HB_ITEMS(8, true) break;
+    case 18: HB_ITEMS(9, false) break;
     default: return cudaErrorInvalidValue;
     }
 #undef HB_ITEMS
@@ -607,6 +617,7 @@ cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *grid_
     case 12: HB_BIG(6, false) break;
     case 13: HB_BIG(6, true) break;
     case 16: HB_BIG(8, false) break;
+    case 18: HB_BIG(9, false) break;
     default: HB_BIG(8, true) break;
     }
 #undef HB_BIG
@@ -623,6 +634,7 @@ cudaError_t integrator_assign(int order, double *jp, double *dt, const double *f
     case 4: assign_kernel<4><<<g, 128, 0, s>>>(jp, dt, force, n, set_dt, eta_s, dtmax); break;
     case 6: assign_kernel<6><<<g, 128, 0, s>>>(jp, dt, force, n, set_dt, eta_s, dtmax); break;
     case 8: assign_kernel<8><<<g, 128, 0, s>>>(jp, dt, force, n, set_dt, eta_s, dtmax); break;
+    case 9: assign_kernel<9><<<g, 128, 0, s>>>(jp, dt, force, n, set_dt, eta_s, dtmax); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -635,6 +647,7 @@ cudaError_t integrator_energy(int order, const double *jp, const double *pot, in
     case 4: energy_partial_kernel<4><<<kEnergyBlocks, 256, 0, s>>>(jp, pot, n, part); break;
     case 6: energy_partial_kernel<6><<<kEnergyBlocks, 256, 0, s>>>(jp, pot, n, part); break;
     case 8: energy_partial_kernel<8><<<kEnergyBlocks, 256, 0, s>>>(jp, pot, n, part); break;
+    case 9: energy_partial_kernel<9><<<kEnergyBlocks, 256, 0, s>>>(jp, pot, n, part); break;
     default: return cudaErrorInvalidValue;
     }
     energy_final_kernel<<<1, 32, 0, s>>>(part, kEnergyBlocks, out);

@@ -47,11 +47,14 @@ __device__ __forceinline__ double rsqrt_fp64(double x)
 
 // ---------------------------------------------------------------------------
 // Predictor: slot record -> position, velocity [, acceleration [, jerk]] at
-// tsys, Horner form with c_k = dt/k.
+// tsys, Horner form with c_k = dt/k.  ORDER 9 (double-double positions, the
+// reference's GPredictor of SRC/hermite8dd.h:284-314): x is the unchanged
+// high part posH, xl the low part posL advanced by the 8th-order Taylor
+// series.
 template <int ORDER>
 __device__ __forceinline__ void predict_slot(const double *r, double tsys,
                                              double x[3], double v[3],
-                                             double a[3], double jk[3])
+                                             double a[3], double jk[3], double *xl = nullptr)
 {
     const double dt = tsys - r[7];
     const double c2 = dt * (1.0 / 2.0), c3 = dt * (1.0 / 3.0);
@@ -71,7 +74,12 @@ __device__ __forceinline__ void predict_slot(const double *r, double tsys,
         } else {
             const double s0 = r[14 + k], k0 = r[17 + k];
             const double d4 = r[20 + k], d5 = r[23 + k];
-            x[k] = p0 + dt * (v0 + c2 * (a0 + c3 * (j0 + c4 * (s0 + c5 * (k0 + c6 * (d4 + c7 * d5))))));
+            if constexpr (ORDER == 9) {
+                x[k] = p0;
+                xl[k] = r[kRecPosL + k] + dt * (v0 + c2 * (a0 + c3 * (j0 + c4 * (s0 + c5 * (k0 + c6 * (d4 + c7 * d5))))));
+            } else {
+                x[k] = p0 + dt * (v0 + c2 * (a0 + c3 * (j0 + c4 * (s0 + c5 * (k0 + c6 * (d4 + c7 * d5))))));
+            }
             v[k] = v0 + dt * (a0 + c2 * (j0 + c3 * (s0 + c4 * (k0 + c5 * (d4 + c6 * d5)))));
             a[k] = a0 + dt * (j0 + c2 * (s0 + c3 * (k0 + c4 * (d4 + c5 * d5))));
             jk[k] = j0 + dt * (s0 + c2 * (k0 + c3 * (d4 + c4 * d5)));
@@ -83,7 +91,7 @@ __device__ __forceinline__ void predict_slot(const double *r, double tsys,
 // FP64 pair interaction.  `I` holds the i-particle, `J` the j-particle
 // (x[3], m, v[3], a[3], jk[3]); f accumulates acc, jrk [, snp [, crk]].
 struct Body64 {
-    double x[3], m, v[3], a[3], jk[3];
+    double x[3], m, v[3], a[3], jk[3], xl[3];   // xl: ORDER 9 only
 };
 
 template <int ORDER>
@@ -92,10 +100,20 @@ __device__ __forceinline__ void interact64(const Body64 &I, const Body64 &J,
 {
     double dr[3], dv[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) { dr[k] = J.x[k] - I.x[k]; dv[k] = J.v[k] - I.v[k]; }
+    for (int k = 0; k < 3; ++k) {
+        if constexpr (ORDER == 9)   // (posHj - posHi) + (posLj - posLi), SRC/hermite8dd.h:358
+            dr[k] = (J.x[k] - I.x[k]) + (J.xl[k] - I.xl[k]);
+        else
+            dr[k] = J.x[k] - I.x[k];
+        dv[k] = J.v[k] - I.v[k];
+    }
     const double r2 = fma(dr[2], dr[2], fma(dr[1], dr[1], fma(dr[0], dr[0], eps2)));
     const double rv = fma(dr[2], dv[2], fma(dr[1], dv[1], dr[0] * dv[0]));
-    const double ri = rsqrt_fp64(r2);
+    double ri;
+    if constexpr (ORDER == 9)       // pairs at zero separation are skipped (SRC/hermite8dd.h:362)
+        ri = r2 == eps2 ? 0.0 : rsqrt_fp64(r2);
+    else
+        ri = rsqrt_fp64(r2);
     const double ri2 = ri * ri;
     const double mr3 = J.m * ri * ri2;
     const double al = rv * ri2;              // alpha = (r.v)/r^2
@@ -119,7 +137,7 @@ __device__ __forceinline__ void interact64(const Body64 &I, const Body64 &J,
             u[k] = fma(-3.0 * be, dr[k], fma(-6.0 * al, t[k], da[k]));
             f[6 + k] = fma(mr3, u[k], f[6 + k]);
         }
-        if constexpr (ORDER == 8) {
+        if constexpr (ORDER >= 8) {
             double dj[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) dj[k] = J.jk[k] - I.jk[k];

@@ -33,7 +33,10 @@ predict_kernel(const double *__restrict__ jp, int n, int npad, double tsys,
         }
         __syncthreads();
         if (tid == 0) {
-            const uint32_t bytes = (uint32_t)(cnt * R * 8);
+            // a bulk copy moves a multiple of 16 bytes: with 29-word records
+            // (ORDER 9) a partial last block rounds up by 8 bytes, which stay
+            // inside the padded record array and the staging buffer
+            const uint32_t bytes = (uint32_t)((cnt * R * 8 + 15) & ~15);
             mbar_arrive_expect_tx(&bar, bytes);
             bulk_load(rec, jp + (size_t)base * R, bytes, &bar);
         }
@@ -48,10 +51,10 @@ predict_kernel(const double *__restrict__ jp, int n, int npad, double tsys,
     }
     const int slot = base + tid;
     if (slot >= npad) return;
-    double x[3], v[3], a[3] = {0, 0, 0}, jk[3] = {0, 0, 0}, m;
+    double x[3], v[3], a[3] = {0, 0, 0}, jk[3] = {0, 0, 0}, xl[3] = {0, 0, 0}, m;
     if (tid < cnt) {
         const double *r = rec + tid * R;
-        predict_slot<ORDER>(r, tsys, x, v, a, jk);
+        predict_slot<ORDER>(r, tsys, x, v, a, jk, xl);
         m = r[3];
     } else {
         for (int k = 0; k < 3; ++k) { x[k] = pad_position(slot, k); v[k] = 0.0; }
@@ -79,7 +82,8 @@ predict_kernel(const double *__restrict__ jp, int n, int npad, double tsys,
             c[(P64_X + k) * 32] = x[k];
             c[(P64_V + k) * 32] = v[k];
             if constexpr (ORDER >= 6) c[(P64_A + k) * 32] = a[k];
-            if constexpr (ORDER == 8) c[(P64_J + k) * 32] = jk[k];
+            if constexpr (ORDER >= 8) c[(P64_J + k) * 32] = jk[k];
+            if constexpr (ORDER == 9) c[(P64_XL + k) * 32] = xl[k];
         }
         c[P64_M * 32] = m;
     }
@@ -104,6 +108,7 @@ cudaError_t launch_predict(int order, bool mixed, const double *jp, int n, int n
     case 13: return launch_predict_t<6, true>(jp, n, npad, tsys, pred, err, s);
     case 16: return launch_predict_t<8, false>(jp, n, npad, tsys, pred, err, s);
     case 17: return launch_predict_t<8, true>(jp, n, npad, tsys, pred, err, s);
+    case 18: return launch_predict_t<9, false>(jp, n, npad, tsys, pred, err, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -115,38 +120,54 @@ cudaError_t launch_predict(int order, bool mixed, const double *jp, int n, int n
 // same bulk-copy ring as the force kernel.  Each 32-slot chunk is summed
 // separately and then added to the running total (two-level blocked sum;
 // the reference uses a four-level cascade, SRC/pot-titan.hu:103-114).
+// ORDER 9 (double-double positions) packs (x, y, z, m, xL, yL, zL) and takes
+// the separation as (xj - xi) + (xLj - xLi) (calc_potential,
+// SRC/hermite8dd.h:397-416).
+template <int ORDER> constexpr int posm_comps() { return ORDER == 9 ? 7 : 4; }
+
 template <int ORDER>
 __global__ void pack_posm_kernel(const double *__restrict__ jp, int n, int npad,
                                  double *__restrict__ posm)
 {
-    constexpr int R = Rec<ORDER>::words;
+    constexpr int R = Rec<ORDER>::words, NC = posm_comps<ORDER>();
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= npad) return;
-    double *c = posm + (size_t)(slot >> 5) * 4 * 32 + (slot & 31);
+    double *c = posm + (size_t)(slot >> 5) * NC * 32 + (slot & 31);
     if (slot < n) {
         const double *r = jp + (size_t)slot * R;
         for (int k = 0; k < 4; ++k) c[k * 32] = r[k];
+        if constexpr (NC == 7)
+            for (int k = 0; k < 3; ++k) c[(4 + k) * 32] = r[kRecPosL + k];
     } else {
         for (int k = 0; k < 3; ++k) c[k * 32] = pad_position(slot, k);
         c[3 * 32] = 0.0;
+        if constexpr (NC == 7)
+            for (int k = 0; k < 3; ++k) c[(4 + k) * 32] = 0.0;
     }
 }
 
 constexpr int kPotThreads = 128;
 constexpr int kPotTileChunks = 8;
-constexpr int kPosmChunkBytes = 4 * 32 * 8;
 
+template <int NC>
 __global__ void __launch_bounds__(kPotThreads)
 potential_kernel(const double *__restrict__ posm, int nchunk, int n, double eps2,
                  double *__restrict__ pot, int *err)
 {
+    constexpr int kPosmChunkBytes = NC * 32 * 8;
     constexpr int TB = kPotTileChunks * kPosmChunkBytes;
     __shared__ __align__(128) unsigned char ring[2 * TB];
     __shared__ __align__(8) uint64_t bar[2];
     const int tid = threadIdx.x;
     const int i = blockIdx.x * kPotThreads + tid;   // < npad always
-    const double *ci = posm + (size_t)(i >> 5) * 4 * 32 + (i & 31);
+    const double *ci = posm + (size_t)(i >> 5) * NC * 32 + (i & 31);
     const double xi = ci[0], yi = ci[32], zi = ci[64];
+    double xli = 0.0, yli = 0.0, zli = 0.0;
+    if constexpr (NC == 7) {
+        xli = ci[128];
+        yli = ci[160];
+        zli = ci[192];
+    }
     const int ntile = (nchunk + kPotTileChunks - 1) / kPotTileChunks;
 
     if (tid == 0) {
@@ -180,12 +201,17 @@ potential_kernel(const double *__restrict__ posm, int nchunk, int n, double eps2
         const int cnt = min(kPotTileChunks, nchunk - t * kPotTileChunks);
         const double *tile = reinterpret_cast<const double *>(ring + (t & 1) * TB);
         for (int q = 0; q < cnt; ++q) {
-            const double *cp = tile + q * 4 * 32;
+            const double *cp = tile + q * NC * 32;
             const int jbase = (t * kPotTileChunks + q) * 32;
             double part = 0.0;
 #pragma unroll 8
             for (int jl = 0; jl < 32; ++jl) {
-                const double dx = cp[jl] - xi, dy = cp[32 + jl] - yi, dz = cp[64 + jl] - zi;
+                double dx = cp[jl] - xi, dy = cp[32 + jl] - yi, dz = cp[64 + jl] - zi;
+                if constexpr (NC == 7) {
+                    dx = dx + (cp[128 + jl] - xli);
+                    dy = dy + (cp[160 + jl] - yli);
+                    dz = dz + (cp[192 + jl] - zli);
+                }
                 const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
                 const double mj = (jbase + jl == i) ? 0.0 : cp[96 + jl];
                 part = fma(-mj, rsqrt_fp64(r2), part);
@@ -206,11 +232,15 @@ cudaError_t launch_potential(int order, const double *jp, int n, int npad, doubl
     case 4: pack_posm_kernel<4><<<g, 128, 0, s>>>(jp, n, npad, posm); break;
     case 6: pack_posm_kernel<6><<<g, 128, 0, s>>>(jp, n, npad, posm); break;
     case 8: pack_posm_kernel<8><<<g, 128, 0, s>>>(jp, n, npad, posm); break;
+    case 9: pack_posm_kernel<9><<<g, 128, 0, s>>>(jp, n, npad, posm); break;
     default: return cudaErrorInvalidValue;
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    potential_kernel<<<npad / kPotThreads, kPotThreads, 0, s>>>(posm, npad / 32, n, eps2, pot, err);
+    if (order == 9)
+        potential_kernel<7><<<npad / kPotThreads, kPotThreads, 0, s>>>(posm, npad / 32, n, eps2, pot, err);
+    else
+        potential_kernel<4><<<npad / kPotThreads, kPotThreads, 0, s>>>(posm, npad / 32, n, eps2, pot, err);
     return cudaGetLastError();
 }
 

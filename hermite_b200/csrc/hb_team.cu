@@ -217,7 +217,8 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
             for (int a = lane; a < kp; a += 32) {
                 const double *r = rec + (size_t)cand[a] * R;
                 double x[3], v[3], ac[3] = {0.0, 0.0, 0.0}, jk[3] = {0.0, 0.0, 0.0};
-                predict_slot<ORDER>(r, m, x, v, ac, jk);
+                double xl[3] = {0.0, 0.0, 0.0};
+                predict_slot<ORDER>(r, m, x, v, ac, jk, xl);
                 const double mass = r[3];
                 const int g = rank * KM + a;
                 const int off = (g >> 5) * P * 32 + (g & 31);
@@ -228,7 +229,8 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
                         d[(P64_X + kk) * 32] = x[kk];
                         d[(P64_V + kk) * 32] = v[kk];
                         if constexpr (ORDER >= 6) d[(P64_A + kk) * 32] = ac[kk];
-                        if constexpr (ORDER == 8) d[(P64_J + kk) * 32] = jk[kk];
+                        if constexpr (ORDER >= 8) d[(P64_J + kk) * 32] = jk[kk];
+                        if constexpr (ORDER == 9) d[(P64_XL + kk) * 32] = xl[kk];
                     }
                     d[P64_M * 32] = mass;
                 }
@@ -276,9 +278,10 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
             for (int q = tid; q < JL; q += T) {
                 const int slot = lo + q;
                 double x[3], v[3], a[3] = {0.0, 0.0, 0.0}, jk[3] = {0.0, 0.0, 0.0}, mass;
+                double xl[3] = {0.0, 0.0, 0.0};
                 if (slot < n) {
                     const double *r = rec + (size_t)q * R;
-                    predict_slot<ORDER>(r, tnext, x, v, a, jk);
+                    predict_slot<ORDER>(r, tnext, x, v, a, jk, xl);
                     mass = r[3];
                 } else {
 #pragma unroll
@@ -291,7 +294,8 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
                     c[(P64_X + k) * 32] = x[k];
                     c[(P64_V + k) * 32] = v[k];
                     if constexpr (ORDER >= 6) c[(P64_A + k) * 32] = a[k];
-                    if constexpr (ORDER == 8) c[(P64_J + k) * 32] = jk[k];
+                    if constexpr (ORDER >= 8) c[(P64_J + k) * 32] = jk[k];
+                    if constexpr (ORDER == 9) c[(P64_XL + k) * 32] = xl[k];
                 }
                 c[P64_M * 32] = mass;
             }
@@ -525,6 +529,7 @@ cudaError_t team_setup(int order, int ctas, TeamConfig *cfg)
     case 4: return team_setup_t<4>(ctas, cfg);
     case 6: return team_setup_t<6>(ctas, cfg);
     case 8: return team_setup_t<8>(ctas, cfg);
+    case 9: return team_setup_t<9>(ctas, cfg);
     }
     return cudaErrorInvalidValue;
 }
@@ -535,6 +540,7 @@ int team_shape(int order, const TeamConfig &cfg, int nmax, TeamLaunch *L)
     case 4: return team_shape_t<4>(cfg, nmax, L);
     case 6: return team_shape_t<6>(cfg, nmax, L);
     case 8: return team_shape_t<8>(cfg, nmax, L);
+    case 9: return team_shape_t<9>(cfg, nmax, L);
     }
     return -1;
 }
@@ -545,6 +551,7 @@ cudaError_t team_launch(int order, const TeamLaunch &L, int teams, cudaStream_t 
     case 4: return team_launch_t<4>(L, teams, s);
     case 6: return team_launch_t<6>(L, teams, s);
     case 8: return team_launch_t<8>(L, teams, s);
+    case 9: return team_launch_t<9>(L, teams, s);
     }
     return cudaErrorInvalidValue;
 }

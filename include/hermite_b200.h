@@ -52,10 +52,18 @@ enum hb_status {
 };
 
 enum hb_precision {
-    HB_FP64 = 0,  /* plain FP64 interaction and accumulation (the judge)     */
-    HB_MIXED = 1  /* FP64 predictor; hi/lo FP32 relative positions; FP32
-                     interaction; FP32 partial sums flushed into FP64
-                     accumulators; FP64 crackle accumulation at 8th order    */
+    HB_FP64 = 0,    /* plain FP64 interaction and accumulation (the judge)   */
+    HB_MIXED = 1,   /* FP64 predictor; hi/lo FP32 relative positions; FP32
+                       interaction; FP32 partial sums flushed into FP64
+                       accumulators; FP64 crackle accumulation at 8th order  */
+    HB_FP64_DD = 2  /* order 8 only: positions as double-double (posH +
+                       posL), the reference's SRC/hermite8dd.h.  Records are
+                       the 8th-order record followed by posL[3] (29 words;
+                       hb_set_jp's derivs: acc jrk snp crk d4a d5a posL);
+                       the predictor advances posL only; pair separations
+                       are (posHj - posHi) + (posLj - posLi), pairs at zero
+                       separation are skipped; FP64 arithmetic otherwise.
+                       The file helpers below take order code 9 for it.  */
 };
 
 /* Gravity(int nbody) -- SRC/hermite4-titan.h:49-57 (also 6th/8th).

@@ -5,7 +5,8 @@ bench.py may import this package.  It never stands in for the product: the
 product path (hermite_b200) has no CPU fallback.
 
 * `Oracle`      -- the scalar FP64 C restatement (oracle/hermite_oracle.c) of the
-                   reference's generic Gravity (SRC/hermite{4,6,8}.h).
+                   reference's generic Gravity (SRC/hermite{4,6,8}.h; order code
+                   9: SRC/hermite8dd.h, double-double positions).
 * `RefGravity`  -- the reference's OWN Gravity (generic or AVX backend),
                    compiled from its sources by oracle/Makefile into oracle/_ref/.
 """
@@ -27,7 +28,8 @@ def record_words(order):
 
 
 def predicted_words(order):
-    return 7 + 3 * (order // 2 - 2)
+    # order code 9: the 8th order with double-double positions (+ posL)
+    return 7 + 3 * (order // 2 - 2) + (3 if order == 9 else 0)
 
 
 def force_words(order):

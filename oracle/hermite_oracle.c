@@ -26,8 +26,14 @@
 #include <math.h>
 #include <stddef.h>
 
+/*
+ * Order code 9 is the 8th order with double-double positions, the
+ * reference's SRC/hermite8dd.h: the record is the 8th-order record followed
+ * by posL[3] (29 doubles), the predicted record the 8th-order one (posH as
+ * the position) followed by the predicted posL[3] (16 doubles).
+ */
 static int rec_words(int order)  { return 8 + 3 * (order - 2); }
-static int pred_words(int order) { return 7 + 3 * (order / 2 - 2); }
+static int pred_words(int order) { return 7 + 3 * (order / 2 - 2) + (order == 9 ? 3 : 0); }
 static int force_words(int order){ return 3 * (order / 2); }
 
 int oracle_record_words(int order)    { return rec_words(order); }
@@ -67,15 +73,22 @@ void oracle_predict(int order, int n, const double *rec, double tsys,
             } else {
                 const double s = p[14 + k], c = p[17 + k];
                 const double d4 = p[20 + k], d5 = p[23 + k];
-                x = pos[k] + dt * (vel[k] + c2 * (acc[k] + c3 * (jrk[k] + c4 * (s + c5 * (c + c6 * (d4 + c7 * d5))))));
+                /* order 9: posH unchanged, posL advanced (SRC/hermite8dd.h:304-306) */
+                const double x0 = order == 9 ? p[26 + k] : pos[k];
+                x = x0 + dt * (vel[k] + c2 * (acc[k] + c3 * (jrk[k] + c4 * (s + c5 * (c + c6 * (d4 + c7 * d5))))));
                 v = vel[k] + dt * (acc[k] + c2 * (jrk[k] + c3 * (s + c4 * (c + c5 * (d4 + c6 * d5)))));
                 a = acc[k] + dt * (jrk[k] + c2 * (s + c3 * (c + c4 * (d4 + c5 * d5))));
                 jj = jrk[k] + dt * (s + c2 * (c + c3 * (d4 + c4 * d5)));
             }
-            q[k] = x;
+            if (order == 9) {
+                q[k] = pos[k];
+                q[13 + k] = x;
+            } else {
+                q[k] = x;
+            }
             q[4 + k] = v;
             if (order >= 6) q[7 + k] = a;
-            if (order == 8) q[10 + k] = jj;
+            if (order >= 8) q[10 + k] = jj;
         }
         q[3] = p[3];
     }
@@ -106,12 +119,14 @@ void oracle_force(int order, int n, const double *pred, int nact, double eps2,
             const double *pj = pred + (size_t)j * P;
             double dr[3], dv[3], da[3] = {0, 0, 0}, dj[3] = {0, 0, 0};
             for (int k = 0; k < 3; k++) {
-                dr[k] = pj[k] - pi[k];
+                /* order 9: (posHj - posHi) + (posLj - posLi), SRC/hermite8dd.h:358 */
+                dr[k] = order == 9 ? (pj[k] - pi[k]) + (pj[13 + k] - pi[13 + k]) : pj[k] - pi[k];
                 dv[k] = pj[4 + k] - pi[4 + k];
                 if (order >= 6) da[k] = pj[7 + k] - pi[7 + k];
-                if (order == 8) dj[k] = pj[10 + k] - pi[10 + k];
+                if (order >= 8) dj[k] = pj[10 + k] - pi[10 + k];
             }
             const double r2 = eps2 + dot3(dr, dr);
+            if (order == 9 && r2 == eps2) continue;   /* SRC/hermite8dd.h:362 */
             const double drdv = dot3(dr, dv);
             const double ri2 = 1.0 / r2;
             const double mri3 = pj[3] * ri2 * sqrt(ri2);
@@ -126,7 +141,7 @@ void oracle_force(int order, int n, const double *pred, int nact, double eps2,
                 const double alpha = drdv * ri2;
                 const double beta = (dvdv + drda) * ri2 + alpha * alpha;
                 double gamma = 0.0;
-                if (order == 8) {
+                if (order >= 8) {
                     const double dvda = dot3(dv, da), drdj = dot3(dr, dj);
                     gamma = (3.0 * dvda + drdj) * ri2
                           + alpha * (3.0 * beta - 4.0 * alpha * alpha);
@@ -137,7 +152,7 @@ void oracle_force(int order, int n, const double *pred, int nact, double eps2,
                     f[3 + k] += mri3 * t1;
                     const double t2 = da[k] + (-6.0 * alpha) * t1 + (-3.0 * beta) * dr[k];
                     f[6 + k] += mri3 * t2;
-                    if (order == 8) {
+                    if (order >= 8) {
                         const double t3 = dj[k] + (-9.0 * alpha) * t2
                                         + (-9.0 * beta) * t1 + (-3.0 * gamma) * dr[k];
                         f[9 + k] += mri3 * t3;
@@ -166,6 +181,8 @@ void oracle_potential(int order, int n, const double *rec, double eps2,
             if (j == i) continue;
             const double *pj = rec + (size_t)j * R;
             double dr[3] = {pj[0] - pi[0], pj[1] - pi[1], pj[2] - pi[2]};
+            if (order == 9)   /* SRC/hermite8dd.h:405-407 */
+                for (int k = 0; k < 3; k++) dr[k] = dr[k] + (pj[26 + k] - pi[26 + k]);
             const double r2 = eps2 + dot3(dr, dr);
             s -= pj[3] / sqrt(r2);
         }

@@ -8,7 +8,8 @@
 // Built by oracle/Makefile into oracle/_ref/ (git-ignored); never shipped as
 // part of the product.
 //
-// Compile with -I<reference>/SRC and exactly one of -DREF_ORDER=4|6|8, and
+// Compile with -I<reference>/SRC and exactly one of -DREF_ORDER=4|6|8|9 (9: the
+// 8th order with double-double positions, SRC/hermite8dd.h), and
 // optionally -DAVX_GRAVITY (the reference's AVX backend, SRC/hermite*-avx.h).
 #include <cstdio>
 #include <cstdlib>
@@ -28,8 +29,10 @@ typedef double v4df __attribute__((vector_size(32)));
 #include "hermite6.h"
 #elif REF_ORDER == 8
 #include "hermite8.h"
+#elif REF_ORDER == 9
+#include "hermite8dd.h"   // 8th order, double-double positions
 #else
-#error "REF_ORDER must be 4, 6 or 8"
+#error "REF_ORDER must be 4, 6, 8 or 9"
 #endif
 
 namespace {
@@ -45,12 +48,17 @@ struct RefCtx {
 
 Particle make_particle(const double *r)
 {
-    // record: pos[3] mass vel[3] tlast derivs[3*(order-2)]
+    // record: pos[3] mass vel[3] tlast derivs[3*(order-2)]; order 9: the
+    // 8th-order record, then posL[3]
     Particle p(0, r[3], dvec3(r[0], r[1], r[2]), dvec3(r[4], r[5], r[6]));
     p.tlast = r[7];
     dvec3 *d = &p.acc;   // acc, jrk, snp, crk, d4a, d5a are contiguous
-    for (int k = 0; k < kOrder - 2; k++)
+    const int nd = kOrder == 9 ? 6 : kOrder - 2;
+    for (int k = 0; k < nd; k++)
         d[k] = dvec3(r[8 + 3 * k], r[9 + 3 * k], r[10 + 3 * k]);
+#if REF_ORDER == 9
+    p.posL = dvec3(r[26], r[27], r[28]);
+#endif
     return p;
 }
 }  // namespace

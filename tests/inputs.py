@@ -10,7 +10,14 @@ DERIV_SCALES = (1.0, 3.0, 10.0, 30.0, 100.0, 300.0)   # acc, jrk, snp, crk, d4a,
 
 def make_records(order: int, n: int, seed: int = 1, masses=None) -> np.ndarray:
     """Records at tlast = -dt_i (dt_i a power of two up to 1/32, or 0), so that
-    predicting to tsys = 0 exercises every term of the Taylor series."""
+    predicting to tsys = 0 exercises every term of the Taylor series.  Order
+    code 9 (8th order, double-double positions): the 8th-order records with a
+    low position part posL of the size of a double's rounding of pos."""
+    if order == 9:
+        rec = make_records(8, n, seed, masses)
+        rng = np.random.default_rng(seed + 104729)
+        posl = rec[:, 0:3] * rng.uniform(-2.0 ** -53, 2.0 ** -53, (n, 3))
+        return np.ascontiguousarray(np.concatenate([rec, posl], axis=1))
     snap = plummer(n, seed, masses=masses)
     rng = np.random.default_rng(seed + 7919)
     nd = order - 2

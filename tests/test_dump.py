@@ -25,7 +25,8 @@ ETA = {4: (0.1, 0.01), 6: (0.5, 0.1), 8: (0.75, 0.1)}
 
 
 def ref_app(order):
-    app = ROOT / "oracle" / "_ref" / f"avx2-{order}"
+    # order code 9: the reference's integrator with double-double positions
+    app = ROOT / "oracle" / "_ref" / ("generic-8dd" if order == 9 else f"avx2-{order}")
     if not app.exists() or not GEN_PLUM.exists():
         pytest.skip("the reference's integrator is not built (needs the reference sources)")
     return app
@@ -35,8 +36,8 @@ def run_ref(app, order, workdir, tend, start, dump_interval=None, dumpout=None):
     """Run the reference integrator from a snapshot (start = ("snap", name)) or
     a dump (("dump", name)); returns the mean-nact strings ("%f") it prints
     per log interval (NbodySystem::print_stat)."""
-    eta, eta_s = ETA[order]
-    lines = [f"order {order}", f"eta {eta}", f"eta_s {eta_s}", f"tend {tend!r}", "dtmaxinv 16",
+    eta, eta_s = ETA[min(order, 8)]
+    lines = [f"order {min(order, 8)}", f"eta {eta}", f"eta_s {eta_s}", f"tend {tend!r}", "dtmaxinv 16",
              "kt_for_eps 1.0", "log_interval 0.125", "snap_interval 100.0",
              f"dump_interval {dump_interval or 100.0!r}"]
     lines.append(("snapin " if start[0] == "snap" else "dumpin ") + start[1])
@@ -48,7 +49,7 @@ def run_ref(app, order, workdir, tend, start, dump_interval=None, dumpout=None):
     return re.findall(r"nact : (\S+)", r.stderr)
 
 
-@pytest.mark.parametrize("order", [4, 6, 8])
+@pytest.mark.parametrize("order", [4, 6, 8, 9])
 def test_host_round_trip(order, tmp_path):
     n, R = 37, hb.record_words(order)
     rng = np.random.default_rng(order)
@@ -58,7 +59,7 @@ def test_host_round_trip(order, tmp_path):
     ids = rng.permutation(n) + 1000
     hb.write_dump(tmp_path / "d.dat", order, rec, aux, 0.375, dumpid=7, energies=(-0.25, -0.2501),
                   steps=(12345, 678), ids=ids)
-    d = hb.read_dump(tmp_path / "d.dat")
+    d = hb.read_dump(tmp_path / "d.dat", dd=order == 9)
     assert (d["order"], d["dumpid"], d["nbody"], d["tsys"]) == (order, 7, n, 0.375)
     assert d["energies"] == (-0.25, -0.2501) and d["steps"] == (12345, 678)
     np.testing.assert_array_equal(d["ids"], ids)
@@ -66,15 +67,17 @@ def test_host_round_trip(order, tmp_path):
     np.testing.assert_array_equal(d["aux"], aux)
 
 
-@pytest.mark.parametrize("order", [4, 6, 8])
+@pytest.mark.parametrize("order", [4, 6, 8, 9])
 def test_reference_dump_rewritten_byte_for_byte(order, tmp_path):
     app = ref_app(order)
     subprocess.run([str(GEN_PLUM), "1"], cwd=tmp_path, check=True, capture_output=True)
     run_ref(app, order, tmp_path, 0.125, ("snap", "pl1k.dat"), dump_interval=0.125,
             dumpout="dump%d.dat")
     src = tmp_path / "dump1.dat"
-    d = hb.read_dump(src)
+    d = hb.read_dump(src, dd=order == 9)
     assert d["order"] == order and d["nbody"] == 1024 and d["tsys"] == 0.125
+    if order == 9:
+        assert np.any(d["records"][:, 26:29] != 0.0)     # the low parts are in the file
     hb.write_dump(tmp_path / "again.dat", order, d["records"], d["aux"], d["tsys"],
                   dumpid=d["dumpid"], energies=d["energies"], steps=d["steps"], ids=d["ids"])
     assert (tmp_path / "again.dat").read_bytes() == src.read_bytes()
@@ -101,11 +104,11 @@ def test_read_errors(tmp_path):
 
 
 def _restored_nact(order, path, engine, tend=0.25):
-    d = hb.read_dump(path)
+    d = hb.read_dump(path, dd=order == 9)
     n = d["nbody"]
     eps = 4.0 / n                            # kt_for_eps 1.0 (set_thermal_eps)
-    eta, _ = ETA[order]
-    with hb.Gravity(order, n, "fp64") as g:
+    eta, _ = ETA[min(order, 8)]
+    with hb.Gravity(min(order, 8), n, "dd" if order == 9 else "fp64") as g:
         g.set_engine(engine)
         did, e0, e1 = g.integrator_restore(path, eps * eps, eta, 1.0 / 16)
         assert (did, e0, e1) == (d["dumpid"], *d["energies"])
@@ -119,7 +122,7 @@ def _restored_nact(order, path, engine, tend=0.25):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("engine", ["graph", "team"])
-@pytest.mark.parametrize("order", [4, 6, 8])
+@pytest.mark.parametrize("order", [4, 6, 8, 9])
 def test_restore_agrees_with_reference_restore(order, engine, tmp_path):
     app = ref_app(order)
     subprocess.run([str(GEN_PLUM), "1"], cwd=tmp_path, check=True, capture_output=True)

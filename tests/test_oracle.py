@@ -19,7 +19,7 @@ EPS2 = (1.0 / 256) ** 2
 GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden"
 
 
-@pytest.mark.parametrize("order", [4, 6, 8])
+@pytest.mark.parametrize("order", [4, 6, 8, 9])
 @pytest.mark.parametrize("n", [1, 2, 5, 64, 100])
 def test_bit_exact_vs_reference_generic(order, n, oracle):
     if not ref_available("generic", order):
