@@ -889,9 +889,9 @@ int team_config_for(hb_ctx *ctx, int n, int want_ctas, TeamConfig *cfg)
         if (want_ctas > 0 || ctas <= 8) return fail(ctx, HB_ERR_CUDA, "a team of %d CTAs cannot be scheduled", ctas);
         ctas = 8;
     }
-    if ((long long)((nch + ctas - 1) / ctas) * 32 > cfg->jl_cap)
+    if ((long long)((nch + ctas - 1) / ctas) * 32 > cfg->jl_cap_g)
         return fail(ctx, HB_ERR_TOO_LARGE, "%d slots do not fit a team of %d CTAs (%d slots each)", n,
-                    ctas, cfg->jl_cap);
+                    ctas, cfg->jl_cap_g);
     return HB_OK;
 }
 

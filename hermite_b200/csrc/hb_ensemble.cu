@@ -689,7 +689,11 @@ int build_groups(hb_ens *e)
         }
         for (;;) {
             const TeamConfig *cf = cfg_for(C);
-            if (cf && (long long)((nch + C - 1) / C) * 32 <= cf->jl_cap) break;
+            // the automatic choice takes only clusters whose records fit in
+            // shared memory (larger ones run faster on the lockstep engine:
+            // measured on 256 clusters of N <= 32768, 16.3 s team vs 12.5 s)
+            const int cap = cf ? (e->engine == HB_ENGINE_TEAM ? cf->jl_cap_g : cf->jl_cap) : 0;
+            if (cf && (long long)((nch + C - 1) / C) * 32 <= cap) break;
             if (e->team_ctas > 0 || C >= 16) {
                 C = 0;
                 break;

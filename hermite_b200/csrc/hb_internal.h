@@ -96,7 +96,8 @@ struct TeamState {     // per system, persistent across launches
 };
 struct TeamConfig {
     int ctas;          // CTAs per team (cluster size)
-    int jl_cap;        // slots per CTA that fit in shared memory (rounds of kTeamIMax)
+    int jl_cap;        // slots per CTA with their records in shared memory (rounds of kTeamIMax)
+    int jl_cap_g;      // slots per CTA with the records left in global memory
     int smem;          // dynamic shared memory available per CTA
     int max_teams;     // co-resident teams on this device
 };
@@ -108,6 +109,7 @@ struct TeamLaunch {
     int *next_sys;     // work counter, zero at launch
     int nsys;
     int ctas, jl_cap, im, smem;   // from team_shape
+    bool rsmem;                   // own records copied into shared memory
     double tend, etapow, dtmax;
     long long max_steps;   // per system and launch
 };

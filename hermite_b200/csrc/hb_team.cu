@@ -54,18 +54,24 @@ struct TeamXch {
     int err;      // a corrector of the sender produced a timestep underflow
 };
 
-// Shared-memory carve-up for jl own slots per CTA and im i-states per round.
+// Shared-memory carve-up for jl own slots per CTA and im i-states per round;
+// the own records are in shared memory (RSMEM) or stay in global memory.
 template <int ORDER>
 struct TeamSmem {
     static constexpr int R = Rec<ORDER>::words, P = Pred64<ORDER>::ncomp, F = Frc<ORDER>::words;
     // per i-state: ibuf [P], part [F] (doubles); gq, gc (ints)
     static constexpr size_t per_i = (size_t)(P + F) * 8 + 2 * 4;
-    // per slot: record, predicted state, tlast + dt, dt (doubles); candidate (int)
-    static constexpr size_t per_slot = (size_t)(R + P + 2) * 8 + 4;
+    // per slot: [record], predicted state, tlast + dt, dt (doubles); candidate (int)
+    static constexpr size_t per_slot(bool rsmem) { return (size_t)((rsmem ? R : 0) + P + 2) * 8 + 4; }
     // xa [16], koff [48], misc [4], alignment
     static constexpr size_t fixed = 16 * sizeof(TeamXch) + (48 + 4) * 4 + 64;
-    static size_t bytes(int jl, int im) { return fixed + per_i * (size_t)im + per_slot * (size_t)jl; }
+    static size_t bytes(int jl, int im, bool rsmem)
+    {
+        return fixed + per_i * (size_t)im + per_slot(rsmem) * (size_t)jl;
+    }
 };
+// Smallest round with the records in global memory (larger systems).
+constexpr int kTeamIMinGlobal = 64;
 
 __device__ __forceinline__ double warp_min(double v)
 {
@@ -124,7 +130,7 @@ __device__ __forceinline__ void team_force(const double *ibuf, const double *pre
     if (gi < nr && js == 0) out(gi, f);
 }
 
-template <int ORDER>
+template <int ORDER, bool RSMEM>
 __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
 {
     constexpr int T = kTeamWarps * 32;
@@ -137,8 +143,8 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
     const int KM = IM / C;         // i states one rank pushes per step (its region of ibuf)
 
     extern __shared__ __align__(16) unsigned char smem[];
-    double *rec = reinterpret_cast<double *>(smem);               // [jl_cap][R] own records
-    double *pred = rec + (size_t)jl_cap * R;                      // [jl_cap/32][P][32]
+    double *rec_s = reinterpret_cast<double *>(smem);             // [jl_cap][R] own records (RSMEM)
+    double *pred = rec_s + (RSMEM ? (size_t)jl_cap * R : 0);      // [jl_cap/32][P][32]
     double *ibuf = pred + (size_t)jl_cap * P;                     // [IM/32][P][32] i states
     double *part = ibuf + IM * P;                                 // [IM][F] partial forces
     double *tn = part + IM * F;                                   // [jl_cap] tlast + dt
@@ -168,11 +174,14 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
         const int nch = (n + 31) >> 5;
         const int c0 = (int)((long long)rank * nch / C), c1 = (int)((long long)(rank + 1) * nch / C);
         const int lo = c0 * 32, JL = (c1 - c0) * 32;
+        // own records: a copy in shared memory, or in place in global memory
+        double *rec = RSMEM ? rec_s : jp + (size_t)lo * R;
 
-        for (int e = tid; e < JL * R; e += T) {
-            const int q = e / R, slot = lo + q;
-            rec[e] = slot < n ? jp[(size_t)lo * R + e] : 0.0;
-        }
+        if constexpr (RSMEM)
+            for (int e = tid; e < JL * R; e += T) {
+                const int q = e / R, slot = lo + q;
+                rec[e] = slot < n ? jp[(size_t)lo * R + e] : 0.0;
+            }
         for (int q = tid; q < JL; q += T) {
             const int slot = lo + q;
             if (slot < n) {
@@ -399,8 +408,9 @@ __global__ void __launch_bounds__(kTeamWarps * 32, 1) team_kernel(TeamLaunch L)
             tsys = tnext;
         }
 
-        for (int e = tid; e < JL * R; e += T)
-            if (lo + e / R < n) jp[(size_t)lo * R + e] = rec[e];
+        if constexpr (RSMEM)
+            for (int e = tid; e < JL * R; e += T)
+                if (lo + e / R < n) jp[(size_t)lo * R + e] = rec[e];
         for (int q = tid; q < JL; q += T)
             if (lo + q < n) dtg[lo + q] = dts[q];
         if (rank == 0 && tid == 0) {
@@ -423,18 +433,23 @@ cudaError_t team_setup_t(int ctas, TeamConfig *cfg)
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
     const int avail = optin - 1024;
-    // slots per CTA with the smallest round (kTeamIMax i-states)
+    // slots per CTA: records in shared memory with the smallest round of
+    // kTeamIMax i-states, or records in global memory with kTeamIMinGlobal
     using SM = TeamSmem<ORDER>;
-    int jl_cap = (int)(((long long)avail - (long long)SM::fixed - (long long)SM::per_i * kTeamIMax) /
-                       (long long)SM::per_slot);
-    jl_cap = std::min(jl_cap & ~31, kTeamMaxSlotsPerCta);
+    auto cap = [&](bool rsmem, int im) {
+        const long long c = ((long long)avail - (long long)SM::fixed - (long long)SM::per_i * im) /
+                            (long long)SM::per_slot(rsmem);
+        return (int)std::min<long long>(c & ~31LL, kTeamMaxSlotsPerCta);
+    };
+    const int jl_cap = cap(true, kTeamIMax), jl_cap_g = cap(false, kTeamIMinGlobal);
     if (jl_cap < 32) return cudaErrorInvalidValue;
     const int smem = avail;
-    const void *k = (const void *)&team_kernel<ORDER>;
-    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess && ctas > 8)
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return e;
+    for (const void *k : {(const void *)&team_kernel<ORDER, true>, (const void *)&team_kernel<ORDER, false>}) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess && ctas > 8)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
     cudaLaunchConfig_t lc = {};
     lc.gridDim = dim3(ctas);
     lc.blockDim = dim3(kTeamWarps * 32);
@@ -447,10 +462,11 @@ cudaError_t team_setup_t(int ctas, TeamConfig *cfg)
     lc.attrs = at;
     lc.numAttrs = 1;
     int teams = 0;
-    e = cudaOccupancyMaxActiveClusters(&teams, (void *)&team_kernel<ORDER>, &lc);
+    e = cudaOccupancyMaxActiveClusters(&teams, (void *)&team_kernel<ORDER, true>, &lc);
     if (e != cudaSuccess) return e;
     cfg->ctas = ctas;
     cfg->jl_cap = jl_cap;
+    cfg->jl_cap_g = std::max(jl_cap, jl_cap_g);
     cfg->smem = smem;
     cfg->max_teams = teams;
     return cudaSuccess;
@@ -465,15 +481,17 @@ int team_shape_t(const TeamConfig &cfg, int nmax, TeamLaunch *L)
     using SM = TeamSmem<ORDER>;
     const int nch = (nmax + 31) / 32;
     const int jl = (nch + cfg.ctas - 1) / cfg.ctas * 32;
-    if (jl > cfg.jl_cap) return -1;
-    long long im = ((long long)cfg.smem - (long long)SM::fixed - (long long)SM::per_slot * jl) /
+    const bool rsmem = jl <= cfg.jl_cap;   // records in shared memory when they fit
+    if (!rsmem && jl > cfg.jl_cap_g) return -1;
+    long long im = ((long long)cfg.smem - (long long)SM::fixed - (long long)SM::per_slot(rsmem) * jl) /
                    (long long)SM::per_i;
     im = std::min<long long>(im & ~31LL, kTeamWarps * 32);
-    if (im < kTeamIMax) return -1;
+    if (im < (rsmem ? kTeamIMax : kTeamIMinGlobal)) return -1;
     L->ctas = cfg.ctas;
     L->jl_cap = jl;
     L->im = (int)im;
-    L->smem = (int)SM::bytes(jl, (int)im);
+    L->rsmem = rsmem;
+    L->smem = (int)SM::bytes(jl, (int)im, rsmem);
     return 0;
 }
 
@@ -492,7 +510,8 @@ cudaError_t team_launch_t(const TeamLaunch &L, int teams, cudaStream_t s)
     at[0].val.clusterDim.z = 1;
     lc.attrs = at;
     lc.numAttrs = 1;
-    return cudaLaunchKernelEx(&lc, team_kernel<ORDER>, L);
+    return L.rsmem ? cudaLaunchKernelEx(&lc, team_kernel<ORDER, true>, L)
+                   : cudaLaunchKernelEx(&lc, team_kernel<ORDER, false>, L);
 }
 
 // Single-system bookkeeping: the multi-kernel engine's scheduler <-> the

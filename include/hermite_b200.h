@@ -265,14 +265,16 @@ int hb_ens_init(hb_ens *ens, double tsys, double eta, double eta_s, double dtmax
 /* Engines for hb_ens_run (HB_ENGINE_* as for hb_integrator_set_engine):
  *  HB_ENGINE_GRAPH  lockstep: one global block-step loop over the union of
  *                   all clusters, five kernels per step from a CUDA graph;
- *  HB_ENGINE_TEAM   every cluster that fits a team of up to 16 CTAs on its
- *                   own block-time sequence: one thread-block cluster of
- *                   team_ctas CTAs (0: chosen per cluster from its size)
- *                   integrates one cluster at a time from a device queue,
- *                   largest first (FP64); the clusters that do not fit
- *                   follow on the lockstep engine;
- *  HB_ENGINE_AUTO   the team engine when every cluster fits a team (FP64),
- *                   else the lockstep engine for all (the default).
+ *  HB_ENGINE_TEAM   every cluster that fits a team of up to 16 CTAs (about
+ *                   33k particles at 6th order) on its own block-time
+ *                   sequence: one thread-block cluster of team_ctas CTAs
+ *                   (0: chosen per cluster from its size) integrates one
+ *                   cluster at a time from a device queue, largest first
+ *                   (FP64); the clusters that do not fit follow on the
+ *                   lockstep engine;
+ *  HB_ENGINE_AUTO   the team engine when every cluster fits a team with its
+ *                   records in shared memory (about 11k particles at 6th
+ *                   order), else the lockstep engine for all (the default).
  * Per cluster both engines integrate the same algorithm; a cluster's
  * result does not depend on the other clusters. */
 int hb_ens_set_engine(hb_ens *ens, int engine, int team_ctas);

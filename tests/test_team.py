@@ -44,6 +44,9 @@ def integrate(order, n, engine, ctas=0, tend=1.0 / 8, seed=3, eta=None):
     (4, 3000, 0),          # first steps have > 256 active slots: several rounds
     (6, 4500, 0),          # steps with > 4096 active slots: the graph engine's large-step kernel
     (8, 4200, 0),
+    (4, 4000, 2),          # more slots per CTA than shared memory holds with their records:
+    (6, 3000, 4),          # the records stay in global memory
+    (8, 2000, 2),
 ])
 def test_team_matches_graph_engine(order, n, ctas):
     s_g, rec_g, dt_g, used_g = integrate(order, n, "graph")
