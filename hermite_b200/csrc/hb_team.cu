@@ -98,36 +98,64 @@ __device__ __forceinline__ double team_dtlim(double tnext, double dtmax)
 
 // Partial forces of nr i-particles (ibuf, AoSoA32, at positions idx(gi))
 // against this CTA's JL own predicted slots.  G lanes (a power of two)
-// share one i, each summing every G-th own slot, and their sums meet in a
-// fixed xor-shuffle tree; out(gi, f) is called by the first lane of each
-// group.  NW * 32 / G >= nr i-slots, nr <= NW * 32.
-template <int ORDER, typename Idx, typename Out>
-__device__ __forceinline__ void team_force(const double *ibuf, const double *pred, int JL, int nr,
-                                           double eps2, Idx idx, Out out)
+// share NI i-particles, each lane summing every G-th own slot, and their
+// sums meet in a fixed xor-shuffle tree; out(gi, f) is called by the first
+// lane of each group.  NW * 32 / G * NI >= nr i-slots.
+template <int ORDER, int NI, typename Idx, typename Out>
+__device__ __forceinline__ void team_force_ni(const double *ibuf, const double *pred, int JL, int nr,
+                                              double eps2, Idx idx, Out out)
 {
     constexpr int NW = kTeamWarps, F = Frc<ORDER>::words;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int G = 32;
-    while (G > 1 && NW * (32 / G) < nr) G >>= 1;
-    const int gi = w * (32 / G) + lane / G, js = lane & (G - 1);
-    double f[F];
+    while (G > 1 && NW * (32 / G) * NI < nr) G >>= 1;
+    const int gp = w * (32 / G) + lane / G, js = lane & (G - 1);
+    double f[NI][F];
 #pragma unroll
-    for (int c = 0; c < F; ++c) f[c] = 0.0;
-    if (gi < nr) {
-        const int x = idx(gi);
-        Body64 I;
-        load_i64<ORDER>(ibuf, x >> 5, x & 31, I);
+    for (int n = 0; n < NI; ++n)
+#pragma unroll
+        for (int c = 0; c < F; ++c) f[n][c] = 0.0;
+    if (gp * NI < nr) {
+        Body64 I[NI];
+#pragma unroll
+        for (int n = 0; n < NI; ++n) {
+            const int x = idx(gp * NI + n < nr ? gp * NI + n : gp * NI);   // a missing pair partner repeats the first
+            load_i64<ORDER>(ibuf, x >> 5, x & 31, I[n]);
+        }
 #pragma unroll 2
         for (int j = js; j < JL; j += G) {
             Body64 J;
             load_i64<ORDER>(pred, j >> 5, j & 31, J);
-            interact64<ORDER>(I, J, eps2, f);
+#pragma unroll
+            for (int n = 0; n < NI; ++n) interact64<ORDER>(I[n], J, eps2, f[n]);
         }
     }
     for (int o = G >> 1; o; o >>= 1)
 #pragma unroll
-        for (int c = 0; c < F; ++c) f[c] += __shfl_xor_sync(0xffffffffu, f[c], o);
-    if (gi < nr && js == 0) out(gi, f);
+        for (int n = 0; n < NI; ++n)
+#pragma unroll
+            for (int c = 0; c < F; ++c) f[n][c] += __shfl_xor_sync(0xffffffffu, f[n][c], o);
+    if (js == 0)
+#pragma unroll
+        for (int n = 0; n < NI; ++n)
+            if (gp * NI + n < nr) out(gp * NI + n, f[n]);
+}
+
+// Two i per lane (two independent chains per j load) at 4th order, where the
+// registers allow it, once the round is large enough for the lane groups to
+// stay narrow; one otherwise.  The choice depends on nr only, so every CTA
+// of a team sums in the same order.
+template <int ORDER, typename Idx, typename Out>
+__device__ __forceinline__ void team_force(const double *ibuf, const double *pred, int JL, int nr,
+                                           double eps2, Idx idx, Out out)
+{
+    if constexpr (ORDER == 4) {
+        if (nr > 128) {
+            team_force_ni<ORDER, 2>(ibuf, pred, JL, nr, eps2, idx, out);
+            return;
+        }
+    }
+    team_force_ni<ORDER, 1>(ibuf, pred, JL, nr, eps2, idx, out);
 }
 
 template <int ORDER, bool RSMEM>
