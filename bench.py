@@ -336,6 +336,7 @@ def run_ours(args):
     ref_gpu = reference_gpu_leg() if not args.skip_integrator else None
     ens = ensemble_leg() if not args.skip_integrator else None
     ens_small = small_ensemble_leg() if not args.skip_integrator else None
+    mixed8 = mixed_vs_fp64_o8() if not args.skip_mixed else None
 
     if rank != 0:
         dist_barrier(world)
@@ -355,6 +356,12 @@ def run_ours(args):
         except Exception as e:          # the baseline is reported, not required
             cpu = {"value": None, "unit": UNIT, "cores": host_threads(), "kind": "reference",
                    "sample": f"failed: {e}"}
+    ens_cpu = None
+    if not args.skip_cpu and not args.skip_integrator:
+        try:
+            ens_cpu = ensemble_cpu_leg()
+        except Exception as e:
+            ens_cpu = {"failed": str(e)}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -381,6 +388,8 @@ def run_ours(args):
         "reference_gpu_recompiled": ref_gpu,
         "ensemble": ens,
         "ensemble_small_clusters": ens_small,
+        "mixed_vs_fp64_o8": mixed8,
+        "ensemble_cpu_reference": ens_cpu,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
@@ -425,6 +434,74 @@ def mixed_vs_fp64(dev, stream):
     res["rel_err_vs_fp64"] = {name: {"max": float(err[:, k].max()), "median": float(np.median(err[:, k]))}
                               for k, name in enumerate(("acc", "jrk", "snp"))}
     return res
+
+
+def mixed_vs_fp64_o8(nsample=4096, nrate=32768):
+    """8th order, Plummer N = 1048576, eps = 1/16384 (the 8th-order
+    configuration): per-particle relative errors of the mixed-precision force
+    against the FP64 force on the first nsample particles (against all N),
+    and both kernels' rates on the first nrate particles."""
+    import torch
+    from hermite_b200 import Gravity
+    order, n, eps2 = 8, 1 << 20, (1.0 / 16384) ** 2
+    rec = plummer_records(order, n, seed=11)
+    res = {"order": order, "nbody": n, "eps": 1.0 / 16384, "sample_i": nsample, "rate_i": nrate}
+    forces = {}
+    stream = torch.cuda.Stream()
+    for prec in ("fp64", "mixed"):
+        with torch.cuda.stream(stream):
+            g = Gravity(order, n, prec)
+            g.set_stream(stream.cuda_stream)
+            g.set_jp_records(rec)
+            g.upload()
+            g.predict_all_device(0.0)
+            g.force_device(nrate, eps2)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g.force_device(nrate, eps2)
+            e1.record(stream)
+            stream.synchronize()
+            ms = e0.elapsed_time(e1)
+            g.set_stream(None)
+            forces[prec] = g.calc_force_on_first_nact(nsample, eps2)
+            g.close()
+        res[prec] = {"gint_s": nrate * n / (ms * 1e-3) * 1e-9, "force_ms": ms}
+    res["speedup"] = res["mixed"]["gint_s"] / res["fp64"]["gint_s"]
+    a, b = forces["mixed"].reshape(nsample, 4, 3), forces["fp64"].reshape(nsample, 4, 3)
+    err = np.linalg.norm(a - b, axis=2) / np.linalg.norm(b, axis=2)
+    res["rel_err_vs_fp64"] = {name: {"max": float(err[:, k].max()), "median": float(np.median(err[:, k]))}
+                              for k, name in enumerate(("acc", "jrk", "snp", "crk"))}
+    return res
+
+
+def ensemble_cpu_leg(nclusters=256, tend=1.0 / 16):
+    """The reference's AVX2 integrator (oracle/_ref/avx2-6, all host cores) on
+    a sample of the ensemble leg's clusters -- the smallest, median and
+    largest whose N is a multiple of 4 (the AVX backend works on groups of
+    4) -- over t = 0..tend (one dtmax, the app's shortest run):
+    interactions per second of each run and of the sample (the CPU
+    counterpart of the ensemble's Gint/s)."""
+    from hermite_b200.ic import plummer, power_law_masses
+    from hermite_b200.run_app import APP, run
+    if not Path(str(APP["cpu-ref"]).format(order=6)).exists():
+        return None
+    rng = np.random.default_rng(2024)
+    sizes = [int(round(np.exp(rng.uniform(np.log(1024), np.log(32768))))) for _ in range(nclusters)]
+    by4 = [int(c) for c in np.argsort(sizes) if sizes[c] % 4 == 0]
+    pick = [by4[0], by4[len(by4) // 2], by4[-1]]
+    runs, inter, wall = [], 0.0, 0.0
+    for c in pick:
+        n = sizes[c]
+        snap = plummer(n, seed=c, masses=power_law_masses(n, np.random.default_rng(c)))
+        r = run("c5", "cpu-ref", tend=tend, snapshot=snap, eps=4.0 / n)
+        i = float(r["particle_steps"]) * n
+        runs.append({"cluster": c, "n": n, "app_wtime_s": r.get("app_wtime_s"),
+                     "gint_s": i / r["app_wtime_s"] * 1e-9 if r.get("app_wtime_s") else None})
+        inter += i
+        wall += r.get("app_wtime_s") or 0.0
+    return {"binary": "oracle/_ref/avx2-6 (reference SRC/hermite6-avx.h, built from source)",
+            "cores": os.cpu_count(), "window": f"t = 0..{tend}", "clusters": runs,
+            "gint_s": inter / wall * 1e-9 if wall else None}
 
 
 def run_profile_case(case: str):

@@ -41,6 +41,8 @@ CONFIGS = {
     "c2": dict(order=4, n=65536, eps=1 / 1024, eta=0.01, eta_s=0.0025, dtmaxinv=16, tend=0.25),
     "c3": dict(order=6, n=262144, eps=1 / 4096, eta=0.1, eta_s=0.02, dtmaxinv=32, tend=0.125),
     "c4": dict(order=8, n=1048576, eps=1 / 16384, eta=0.2, eta_s=0.04, dtmaxinv=64, tend=1 / 32),
+    # one cluster of the batched ensemble (its N and eps = 4/N given per run)
+    "c5": dict(order=6, n=1024, eps=4 / 1024, eta=0.1, eta_s=0.02, dtmaxinv=16, tend=0.25),
 }
 
 APP = {"gpu": ROOT / "hermite_b200" / "gravity" / "_build" / "hb-app-{order}",
@@ -58,13 +60,20 @@ def input_text(cfg, snap, log_interval):
 
 
 def run(config: str, impl: str = "gpu", tend: float | None = None, n: int | None = None,
-        seed: int = 0, workdir: Path | None = None, threads: int | None = None) -> dict:
+        seed: int = 0, workdir: Path | None = None, threads: int | None = None,
+        snapshot=None, eps: float | None = None) -> dict:
+    """snapshot: initial conditions (an ic.Snapshot) instead of the seeded
+    Plummer sphere; eps: softening instead of the configuration's."""
     from hermite_b200.ic import plummer, write_snapshot
     cfg = dict(CONFIGS[config])
     if tend is not None:
         cfg["tend"] = tend
     if n is not None:
         cfg["n"] = n
+    if snapshot is not None:
+        cfg["n"] = snapshot.n
+    if eps is not None:
+        cfg["eps"] = eps
     app = Path(str(APP[impl]).format(order=cfg["order"]))
     if not app.exists():
         raise FileNotFoundError(f"{app} not built (needs the reference sources)")
@@ -72,9 +81,13 @@ def run(config: str, impl: str = "gpu", tend: float | None = None, n: int | None
     if workdir is None:
         tmp = tempfile.TemporaryDirectory()
         workdir = Path(tmp.name)
-    snap = workdir / f"plummer_{cfg['n']}_{seed}.dat"
-    if not snap.exists():
-        write_snapshot(snap, plummer(cfg["n"], seed))
+    if snapshot is not None:
+        snap = workdir / f"given_{cfg['n']}.dat"
+        write_snapshot(snap, snapshot)
+    else:
+        snap = workdir / f"plummer_{cfg['n']}_{seed}.dat"
+        if not snap.exists():
+            write_snapshot(snap, plummer(cfg["n"], seed))
     dtmax = 1.0 / cfg["dtmaxinv"]
     log_interval = max(dtmax, cfg["tend"] / 8)
     env = dict(os.environ)
