@@ -34,6 +34,14 @@ constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;   // +inf
 #define HB_BIG_NACT 4096
 #endif
 constexpr int kBigNact = HB_BIG_NACT;
+// Small steps: j-slices of at least this many 32-slot chunks, and a slice
+// count aimed at this percentage of the launch's work-item target.
+#ifndef HB_ITEMS_MIN_CHUNKS
+#define HB_ITEMS_MIN_CHUNKS 8
+#endif
+#ifndef HB_ITEMS_TARGET_PCT
+#define HB_ITEMS_TARGET_PCT 100
+#endif
 
 // Programmatic dependent launch: let the next kernel of the step be
 // scheduled now, then wait until the previous kernel's results are visible.
@@ -102,6 +110,46 @@ __global__ void sched_compact_kernel(const double *__restrict__ jp, const double
     }
 }
 
+// Sum of the S slice partials of one i-tile (V values, slice stride sstride
+// doubles) by the T threads of the last CTA to finish it.  With few values
+// the slices are split among thread groups (g, g+G, g+2G, ...) whose sums
+// are added in group order through red[T]; the order is fixed either way.
+template <int T>
+__device__ __forceinline__ void sum_slices(const double *pbase, size_t sstride, int S, int V,
+                                           double *out, double *red)
+{
+    const int tid = threadIdx.x;
+    if (V >= T / 2) {
+        for (int e = tid; e < V; e += T) {
+            double sum = 0.0;
+            int s = 0;
+            for (; s + 4 <= S; s += 4) {
+                const double p0 = __ldcg(pbase + (size_t)(s + 0) * sstride + e);
+                const double p1 = __ldcg(pbase + (size_t)(s + 1) * sstride + e);
+                const double p2 = __ldcg(pbase + (size_t)(s + 2) * sstride + e);
+                const double p3 = __ldcg(pbase + (size_t)(s + 3) * sstride + e);
+                sum += p0; sum += p1; sum += p2; sum += p3;
+            }
+            for (; s < S; ++s) sum += __ldcg(pbase + (size_t)s * sstride + e);
+            out[e] = sum;
+        }
+    } else {
+        const int G = T / V;
+        const int g = tid / V, e = tid % V;
+        if (g < G) {
+            double sum = 0.0;
+            for (int s = g; s < S; s += G) sum += __ldcg(pbase + (size_t)s * sstride + e);
+            red[tid] = sum;
+        }
+        __syncthreads();
+        if (tid < V) {
+            double sum = red[tid];
+            for (int gg = 1; gg < G; ++gg) sum += red[gg * V + tid];
+            out[tid] = sum;
+        }
+    }
+}
+
 // Fused predict + force over work items (i-tile of 32 active slots, j-slice),
 // taken from a device counter by a grid sized once; one warp per quarter of
 // every j tile (the 32 i are shared by the CTA's 4 warps).
@@ -139,8 +187,9 @@ force_items_kernel(ItemsArgs a)
     const double tsys = a.s->tnext, eps2 = a.s->eps2;
     const int tid = threadIdx.x, lane = tid & 31, jg = tid >> 5;
     const int gx = (nact + TI - 1) / TI;
-    int S = (a.target_items + gx - 1) / gx;
-    S = max(1, min(S, max(1, a.nchunk / 8)));
+    const int target = (int)((long long)a.target_items * HB_ITEMS_TARGET_PCT / 100);
+    int S = (target + gx - 1) / gx;
+    S = max(1, min(S, max(1, a.nchunk / HB_ITEMS_MIN_CHUNKS)));
     while (S > 1 && (size_t)S * gx * TI * F > a.partial_cap) --S;
     const int items = gx * S;
     const size_t ispan = (size_t)gx * TI;
@@ -250,13 +299,9 @@ force_items_kernel(ItemsArgs a)
             __syncthreads();
             if (s_last) {
                 __threadfence();
-                const int V = min(TI, nact - itile * TI) * F;
-                const double *pbase = a.partial + (size_t)itile * TI * F;
-                for (int e = tid; e < V; e += NW * 32) {
-                    double sum = 0.0;
-                    for (int s2 = 0; s2 < S; ++s2) sum += __ldcg(pbase + (size_t)s2 * ispan * F + e);
-                    a.force[(size_t)itile * TI * F + e] = sum;
-                }
+                sum_slices<NW * 32>(a.partial + (size_t)itile * TI * F, ispan * F, S,
+                                    min(TI, nact - itile * TI) * F, a.force + (size_t)itile * TI * F,
+                                    reinterpret_cast<double *>(smem));
                 if (tid == 0) a.counter[itile] = 0u;
             }
         }
@@ -408,13 +453,9 @@ force_items_big_kernel(ItemsArgs a)
             __syncthreads();
             if (s_last) {
                 __threadfence();
-                const int V = min(TI, nact - itile * TI) * F;
-                const double *pbase = a.partial + (size_t)itile * TI * F;
-                for (int e = tid; e < V; e += NW * 32) {
-                    double sum = 0.0;
-                    for (int s2 = 0; s2 < S; ++s2) sum += __ldcg(pbase + (size_t)s2 * ispan * F + e);
-                    a.force[(size_t)itile * TI * F + e] = sum;
-                }
+                sum_slices<NW * 32>(a.partial + (size_t)itile * TI * F, ispan * F, S,
+                                    min(TI, nact - itile * TI) * F, a.force + (size_t)itile * TI * F,
+                                    reinterpret_cast<double *>(smem));
                 if (tid == 0) a.counter[itile] = 0u;
             }
         }
