@@ -8,6 +8,12 @@ library compiles in (hb_capi.cu looks up the nearest bucket).
 
     python -m hermite_b200.autotune [--out hermite_b200/csrc/hb_tuning.inc]
                                     [--json results.json] [--quick]
+                                    [--orders 4,6,8] [--precisions fp64,mixed]
+                                    [--n-buckets 65536] [--nact-buckets 2,8,32]
+                                    [--merge]
+
+--merge keeps the existing table and replaces or adds only the measured
+(order, precision, N bucket, nact bucket) entries.
 
 Timing: CUDA events on the context's stream around back-to-back force
 launches (inputs resident, predicted once), median of the repeats.
@@ -130,6 +136,31 @@ def write_inc(results, path: Path, device_name: str):
     path.write_text("\n".join(lines) + "\n")
 
 
+def merge_inc(results, path: Path, device_name: str):
+    """Replace or add the measured entries in an existing table, keeping its
+    other entries and comment lines; entries stay sorted by key."""
+    comments, table = [], {}
+    for line in path.read_text().splitlines():
+        t = line.strip()
+        if t.startswith("{"):
+            v = [int(x) for x in t.strip("{},").split(",")]
+            table[tuple(v[:4])] = tuple(v[4:])
+        elif t:
+            comments.append(line)
+    keys = []
+    for r in results:
+        k = (r["order"], 1 if r["precision"] == "mixed" else 0, int(round(math.log2(r["n"]))),
+             int(round(math.log2(r["nact"]))))
+        table[k] = (r["variant"], r["jsplit"])
+        keys.append(k)
+    groups = sorted({k[:3] for k in keys})
+    comments.append(f"// {datetime.date.today().isoformat()}, {device_name}: merged "
+                    + ", ".join(f"(order {o}, {'mixed' if m else 'fp64'}, 2^{n})" for o, m, n in groups)
+                    + " at nact 2^" + ",".join(sorted({str(k[3]) for k in keys}, key=int)))
+    lines = comments + ["{%d, %d, %d, %d, %d, %d}," % (*k, *table[k]) for k in sorted(table)]
+    path.write_text("\n".join(lines) + "\n")
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--out", default=str(PKG / "csrc" / "hb_tuning.inc"))
@@ -137,11 +168,18 @@ def main():
     ap.add_argument("--orders", default="4,6,8")
     ap.add_argument("--precisions", default="fp64,mixed")
     ap.add_argument("--quick", action="store_true", help="fewer j-split candidates")
+    ap.add_argument("--n-buckets", default=",".join(map(str, N_BUCKETS)))
+    ap.add_argument("--nact-buckets", default=",".join(map(str, NACT_BUCKETS)))
+    ap.add_argument("--merge", action="store_true", help="update only the measured entries")
     a = ap.parse_args()
     import torch
-    res = tune([int(x) for x in a.orders.split(",")], a.precisions.split(","), N_BUCKETS,
-               NACT_BUCKETS, quick=a.quick)
-    write_inc(res, Path(a.out), torch.cuda.get_device_name(0))
+    res = tune([int(x) for x in a.orders.split(",")], a.precisions.split(","),
+               [int(x) for x in a.n_buckets.split(",")], [int(x) for x in a.nact_buckets.split(",")],
+               quick=a.quick)
+    if a.merge and Path(a.out).exists():
+        merge_inc(res, Path(a.out), torch.cuda.get_device_name(0))
+    else:
+        write_inc(res, Path(a.out), torch.cuda.get_device_name(0))
     if a.json:
         Path(a.json).write_text(json.dumps(res, indent=1))
     print(f"wrote {a.out} ({len(res)} entries)")
