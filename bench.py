@@ -337,6 +337,7 @@ def run_ours(args):
     ens = ensemble_leg() if not args.skip_integrator else None
     ens_small = small_ensemble_leg() if not args.skip_integrator else None
     mixed8 = mixed_vs_fp64_o8() if not args.skip_mixed else None
+    pred = predictor_leg() if not args.skip_mixed else None
 
     if rank != 0:
         dist_barrier(world)
@@ -389,6 +390,7 @@ def run_ours(args):
         "ensemble": ens,
         "ensemble_small_clusters": ens_small,
         "mixed_vs_fp64_o8": mixed8,
+        "predictor_roofline": pred,
         "ensemble_cpu_reference": ens_cpu,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
@@ -434,6 +436,56 @@ def mixed_vs_fp64(dev, stream):
     res["rel_err_vs_fp64"] = {name: {"max": float(err[:, k].max()), "median": float(np.median(err[:, k]))}
                               for k, name in enumerate(("acc", "jrk", "snp"))}
     return res
+
+
+def hbm_peak():
+    """Measured HBM copy bandwidth of this pool's B200s (GB/s), else the
+    earlier measurement on the same pool."""
+    p = Path(__file__).resolve().parent / "MEASURED_PEAKS.json"
+    try:
+        v = json.loads(p.read_text()).get("hbm_gbs")
+        if v:
+            return float(v), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "fallback (6.65 TB/s, earlier copy measurement on this pool)"
+
+
+def predictor_leg(reps=50):
+    """The predictor pass alone (hb_predict_pass), plain FP64, back to back:
+    algorithmic bytes = N x (record read + predicted state written) =
+    168 / 312 B per slot at 4th / 8th order, over the mean CUDA-event time of
+    one pass.  8th order, N = 2^20 moves 327 MB per pass (above L2: HBM
+    bound); 4th order, N = 65536 moves 11 MB (L2 resident, launch bound)."""
+    import torch
+    from hermite_b200 import Gravity
+    peak, src = hbm_peak()
+    out = {"peak_gb_s": peak, "peak_source": src}
+    stream = torch.cuda.Stream()
+    for order, n in ((4, 1 << 16), (8, 1 << 20)):
+        rec = plummer_records(order, n, seed=3)
+        with torch.cuda.stream(stream):
+            g = Gravity(order, n, "fp64")
+            g.set_stream(stream.cuda_stream)
+            g.set_jp_records(rec)
+            g.upload()
+            g.predict_all_device(1e-3)
+            for _ in range(3):
+                g.predict_pass()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                g.predict_pass()
+            e1.record(stream)
+            stream.synchronize()
+            us = e0.elapsed_time(e1) / reps * 1e3
+            g.set_stream(None)
+            g.close()
+        nbytes = n * 8 * ({4: 14, 6: 20, 8: 26}[order] + {4: 7, 6: 10, 8: 13}[order])
+        gbs = nbytes / (us * 1e-6) * 1e-9
+        out[f"order{order}_n{n}"] = {"bytes_per_pass": nbytes, "us_per_pass": us, "gb_s": gbs,
+                                     "frac": gbs / peak}
+    return out
 
 
 def mixed_vs_fp64_o8(nsample=4096, nrate=32768):

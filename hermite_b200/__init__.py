@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "hb_create", "hb_destroy", "hb_set_jp", "hb_set_jp_records", "hb_predict_all",
     "hb_force_first_nact", "hb_potential", "hb_set_precision", "hb_get_precision",
     "hb_last_error", "hb_status_string", "hb_set_stream", "hb_upload",
-    "hb_predict_all_device", "hb_force_device", "hb_download_forces", "hb_device_forces",
+    "hb_predict_all_device", "hb_predict_pass", "hb_force_device", "hb_download_forces", "hb_device_forces",
     "hb_synchronize", "hb_launch_count", "hb_set_force_shape", "hb_force_variant_count",
     "hb_force_variant_info", "hb_measure_fma_peak", "hb_force_predicted_noalloc",
     "hb_integrator_init", "hb_integrator_run", "hb_integrator_stats", "hb_energy",
@@ -151,6 +151,7 @@ def load_library() -> ctypes.CDLL:
         "hb_set_stream": (I, [P, P]),
         "hb_upload": (I, [P]),
         "hb_predict_all_device": (I, [P, D]),
+        "hb_predict_pass": (I, [P]),
         "hb_force_device": (I, [P, I, D]),
         "hb_download_forces": (I, [P, I, dp]),
         "hb_device_forces": (P, [P]),
@@ -309,6 +310,11 @@ class Gravity:
 
     def predict_all_device(self, tsys: float):
         self._check(self._lib.hb_predict_all_device(self._h, float(tsys)), "predict_all_device")
+
+    def predict_pass(self):
+        """Run the predictor pass now (normally it runs with the next
+        two-pass force launch); for timing the predictor alone."""
+        self._check(self._lib.hb_predict_pass(self._h), "predict_pass")
 
     def force_device(self, nact: int, eps2: float):
         self._check(self._lib.hb_force_device(self._h, int(nact), float(eps2)), "force_device")

@@ -507,6 +507,17 @@ int hb_predict_all_device(hb_ctx *ctx, double tsys)
     return HB_OK;
 }
 
+int hb_predict_pass(hb_ctx *ctx)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    if (ctx->pred_precision < 0) return fail(ctx, HB_ERR_STATE, "predictor pass before any predict_all");
+    HB_CK(launch_predict(ctx->order, ctx->pred_precision == HB_MIXED, ctx->d_jp, ctx->nbody, ctx->npad,
+                         ctx->tsys, ctx->d_pred, ctx->d_err, ctx->stream));
+    ctx->launches++;
+    ctx->pred_stale = false;
+    return HB_OK;
+}
+
 int hb_predict_all(hb_ctx *ctx, double tsys)
 {
     if (!ctx) return HB_ERR_INVALID;

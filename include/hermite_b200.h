@@ -127,6 +127,11 @@ int hb_upload(hb_ctx *ctx);
  * The prediction runs with the next force launch (inside the fused force
  * kernel, or as a predictor pass ahead of a two-pass one). */
 int hb_predict_all_device(hb_ctx *ctx, double tsys);
+/* Run the predictor pass now: every slot predicted to the tsys of the last
+ * predict_all into the context's predicted array (the two-pass force shapes
+ * read it; fused shapes predict for themselves).  The next two-pass force
+ * launch then skips its own pass.  For timing the predictor alone. */
+int hb_predict_pass(hb_ctx *ctx);
 /* The kernel part of calc_force_on_first_nact: results stay in HBM
  * (hb_device_forces), nothing is copied back, no synchronisation. */
 int hb_force_device(hb_ctx *ctx, int nact, double eps2);

@@ -160,3 +160,26 @@ def test_deterministic(oracle):
             g.predict_all(0.0)
             outs.append(g.calc_force_on_first_nact(37, EPS2))
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_predictor_pass_on_its_own(precision):
+    """An explicit predictor pass (hb_predict_pass) before a two-pass force
+    leaves the forces unchanged to the bit; before any predict_all it is a
+    state error."""
+    from hermite_b200 import HermiteError
+    order, n, nact = 6, 3000, 500
+    rec = make_records(order, n, seed=17)
+    out = []
+    for explicit in (False, True):
+        with Gravity(order, n, precision) as g:
+            if explicit:
+                with pytest.raises(HermiteError):
+                    g.predict_pass()
+            g.set_force_shape(0, 4)           # a two-pass shape
+            g.set_jp_records(rec)
+            g.predict_all(0.125)
+            if explicit:
+                g.predict_pass()
+            out.append(g.calc_force_on_first_nact(nact, EPS2))
+    assert np.array_equal(out[0], out[1])
