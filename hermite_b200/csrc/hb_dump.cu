@@ -19,8 +19,15 @@
 // 8th) travel in a separate 6-double "aux" row per particle.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <memory>
+
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <string>
 #include <vector>
 
@@ -71,6 +78,286 @@ double recalc_dt(int order, const double *rec, const double *aux, double eta, do
 
 using hb::kAuxWords;
 
+
+// ---------------------------------------------------------------------------
+// "%A" text both ways, for files of millions of particles: the whole file is
+// read into memory, particle lines are split over host threads, and the
+// number forms that printf("%A") writes are converted by exact fast paths,
+// with the C library (strtod, snprintf) for any other text.
+
+namespace {
+
+// A whole file in memory, NUL-terminated (the parsers stop there).
+struct Text {
+    std::unique_ptr<char[]> data;   // not zero-filled
+    size_t size = 0;
+    const char *c_str() const { return data.get(); }
+};
+
+bool slurp(const char *path, Text &buf)
+{
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0) return false;
+    struct stat st;
+    if (::fstat(fd, &st) != 0 || st.st_size < 0) {
+        ::close(fd);
+        return false;
+    }
+    const size_t sz = (size_t)st.st_size;
+    buf.data.reset(new char[sz + 1]);
+    buf.size = sz;
+    buf.data[sz] = '\0';
+    // ranges of at least 8 MiB read by host threads in parallel
+    constexpr size_t kPart = (size_t)8 << 20;
+    const int nt = (int)std::max<size_t>(1, std::min<size_t>(8, sz / kPart));
+    const size_t per = (sz + nt - 1) / nt;
+    int bad = 0;
+#pragma omp parallel for num_threads(nt) schedule(static, 1) reduction(| : bad)
+    for (int t = 0; t < nt; ++t) {
+        size_t o = (size_t)t * per;
+        const size_t e = std::min(sz, o + per);
+        while (o < e) {
+            const ssize_t got = ::pread(fd, buf.data.get() + o, e - o, (off_t)o);
+            if (got <= 0) {
+                bad = 1;
+                break;
+            }
+            o += (size_t)got;
+        }
+    }
+    ::close(fd);
+    return !bad;
+}
+
+inline bool is_blank(char c)
+{
+    return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f';
+}
+
+struct HexTable {
+    signed char v[256];
+    HexTable()
+    {
+        for (int c = 0; c < 256; ++c) v[c] = -1;
+        for (int c = 0; c < 10; ++c) v['0' + c] = (signed char)c;
+        for (int c = 0; c < 6; ++c) v['A' + c] = v['a' + c] = (signed char)(10 + c);
+    }
+};
+const HexTable kHex;
+
+inline int hexdigit(char c) { return kHex.v[(unsigned char)c]; }
+
+// The finite forms printf("%A") writes: [-]0X1[.h..h]P(+|-)d for normal
+// numbers, [-]0X0.h..hP-1022 for subnormals and [-]0X0P+0 for zero, with at
+// most 13 fraction digits.  These digits are the IEEE fraction bits and the
+// exponent the unbiased one, so the double is assembled bit for bit, exactly.
+// Returns the end of the number,
+// or nullptr for any other text (decimal, more digits, NAN, INF, a leading 1
+// with an exponent outside the normal range), which is left to strtod.
+const char *parse_hexA(const char *p, double *out)
+{
+    const bool neg = *p == '-';
+    if (neg || *p == '+') ++p;
+    if (p[0] != '0' || (p[1] != 'X' && p[1] != 'x')) return nullptr;
+    p += 2;
+    const int lead = *p - '0';
+    if (lead != 0 && lead != 1) return nullptr;
+    ++p;
+    uint64_t mant = (uint64_t)lead;
+    int nd = 0;
+    if (*p == '.') {
+        ++p;
+        for (int d; (d = hexdigit(*p)) >= 0; ++p) {
+            if (++nd > 13) return nullptr;
+            mant = (mant << 4) | (uint64_t)d;
+        }
+    }
+    if (*p != 'P' && *p != 'p') return nullptr;
+    ++p;
+    const bool eneg = *p == '-';
+    if (eneg || *p == '+') ++p;
+    if (*p < '0' || *p > '9') return nullptr;
+    int ex = 0;
+    for (; *p >= '0' && *p <= '9'; ++p) {
+        ex = ex * 10 + (*p - '0');
+        if (ex > 100000) return nullptr;
+    }
+    if (eneg) ex = -ex;
+    if (mant == 0) {
+        *out = neg ? -0.0 : 0.0;
+        return p;
+    }
+    if (lead == 1 ? (ex < -1022 || ex > 1023) : ex != -1022) return nullptr;
+    // the IEEE encoding directly: the fraction digits left-aligned in 52 bits
+    // under the biased exponent (0 for subnormals)
+    const uint64_t frac = (mant & ((1ull << (4 * nd)) - 1)) << (52 - 4 * nd);
+    const uint64_t bits = ((uint64_t)neg << 63) | ((uint64_t)(lead ? ex + 1023 : 0) << 52) | frac;
+    std::memcpy(out, &bits, sizeof bits);
+    return p;
+}
+
+// The next number after blanks: the exact fast path, else strtod.
+inline bool next_double(const char *&p, double *v)
+{
+    while (is_blank(*p)) ++p;
+    if (const char *e = parse_hexA(p, v)) {
+        p = e;
+        return true;
+    }
+    char *e = nullptr;
+    *v = std::strtod(p, &e);
+    if (e == p) return false;
+    p = e;
+    return true;
+}
+
+inline bool next_long(const char *&p, long long *v)
+{
+    while (is_blank(*p)) ++p;
+    char *e = nullptr;
+    *v = std::strtoll(p, &e, 10);
+    if (e == p) return false;
+    p = e;
+    return true;
+}
+
+// nbody records of an integer and nv numbers each, from buf[body] on, into
+// ids[i] (if ids) and vals[i * nv + k].  With one record per line (as every
+// writer of these formats lays them out) the lines are parsed in parallel;
+// any other layout is read token by token, as fscanf would.
+bool parse_records(const Text &buf, size_t body, int nbody, int nv, long long *ids,
+                   double *vals)
+{
+    const char *base = buf.c_str();
+    const size_t len = buf.size;
+    std::vector<size_t> start, end;
+    start.reserve((size_t)nbody);
+    end.reserve((size_t)nbody);
+    for (size_t p = body; p < len && (int)start.size() < nbody;) {
+        while (p < len && is_blank(base[p])) ++p;
+        if (p >= len) break;
+        const void *nl = std::memchr(base + p, '\n', len - p);
+        const size_t e = nl ? (size_t)(static_cast<const char *>(nl) - base) : len;
+        start.push_back(p);
+        end.push_back(e);
+        p = e;
+    }
+    bool lines_ok = (int)start.size() == nbody;
+    if (lines_ok) {
+        int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+        for (int i = 0; i < nbody; ++i) {
+            const char *q = base + start[i], *lim = base + end[i];
+            long long id = 0;
+            bool ok = next_long(q, &id);
+            double *v = vals + (size_t)i * nv;
+            for (int k = 0; ok && k < nv; ++k) ok = next_double(q, &v[k]);
+            ok = ok && q <= lim;
+            while (ok && q < lim) ok = is_blank(*q++);
+            if (ids) ids[i] = id;
+            bad |= !ok;
+        }
+        lines_ok = bad == 0;
+    }
+    if (lines_ok) return true;
+    const char *q = base + body;
+    for (int i = 0; i < nbody; ++i) {
+        long long id = 0;
+        if (!next_long(q, &id)) return false;
+        if (ids) ids[i] = id;
+        for (int k = 0; k < nv; ++k)
+            if (!next_double(q, &vals[(size_t)i * nv + k])) return false;
+    }
+    return true;
+}
+
+// printf("%A") of x, character for character as the C library writes it:
+// the fraction's hex digits without trailing zeros, subnormals as
+// 0X0.h..hP-1022, zero as 0X0P+0, NAN and INF with their signs.
+int put_hexA(double x, char *o)
+{
+    uint64_t b;
+    std::memcpy(&b, &x, sizeof b);
+    char *const s = o;
+    if (b >> 63) *o++ = '-';
+    const int eb = (int)((b >> 52) & 0x7ff);
+    uint64_t f = b & ((1ull << 52) - 1);
+    if (eb == 0x7ff) {
+        std::memcpy(o, f ? "NAN" : "INF", 3);
+        return (int)(o + 3 - s);
+    }
+    *o++ = '0';
+    *o++ = 'X';
+    *o++ = eb ? '1' : '0';
+    const int e = eb ? eb - 1023 : (f ? -1022 : 0);
+    if (f) {
+        int nd = 13;
+        while ((f & 0xf) == 0) {
+            f >>= 4;
+            --nd;
+        }
+        *o++ = '.';
+        for (int k = nd - 1; k >= 0; --k) *o++ = "0123456789ABCDEF"[(f >> (4 * k)) & 0xf];
+    }
+    *o++ = 'P';
+    *o++ = e < 0 ? '-' : '+';
+    unsigned a = (unsigned)(e < 0 ? -e : e);
+    char d[8];
+    int n = 0;
+    do {
+        d[n++] = (char)('0' + a % 10);
+        a /= 10;
+    } while (a);
+    while (n) *o++ = d[--n];
+    return (int)(o - s);
+}
+
+// Formats lines [0, nbody) with line(i, out) -> bytes written (at most
+// kMaxLine), in blocks over host threads, and writes them in order.
+constexpr int kMaxLine = 2048;
+
+template <typename LineFn>
+bool write_lines(FILE *fp, int nbody, LineFn line)
+{
+    constexpr int kBlock = 4096;   // lines formatted per task
+    const int nblk = (nbody + kBlock - 1) / kBlock;
+    std::vector<std::unique_ptr<char[]>> out((size_t)nblk);   // not zero-filled
+    std::vector<size_t> used((size_t)nblk, 0);
+#pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < nblk; ++b) {
+        const int i0 = b * kBlock, i1 = std::min(nbody, i0 + kBlock);
+        out[b].reset(new char[(size_t)(i1 - i0) * kMaxLine]);
+        char *o = out[b].get();
+        size_t u = 0;
+        for (int i = i0; i < i1; ++i) u += (size_t)line(i, o + u);
+        used[b] = u;
+    }
+    bool ok = true;
+    for (int b = 0; b < nblk; ++b) ok = ok && std::fwrite(out[b].get(), 1, used[b], fp) == used[b];
+    return ok;
+}
+
+// "%<width>ld" of v.
+inline int put_id(long long v, int width, char *o)
+{
+    return std::snprintf(o, 32, "%*lld", width, v);
+}
+
+// " "-separated groups of three: sep then "%A %A %A".
+inline int put_vec(const char *sep, const double *v, char *o)
+{
+    char *const s = o;
+    for (const char *c = sep; *c; ++c) *o++ = *c;
+    o += put_hexA(v[0], o);
+    *o++ = ' ';
+    o += put_hexA(v[1], o);
+    *o++ = ' ';
+    o += put_hexA(v[2], o);
+    return (int)(o - s);
+}
+
+}  // namespace
+
 extern "C" {
 
 int hb_dump_write(const char *path, int order, int dumpid, int nbody, double tsys,
@@ -87,19 +374,22 @@ int hb_dump_write(const char *path, int order, int dumpid, int nbody, double tsy
     std::fprintf(fp, "%d %d\n%ld\n%20.16f\n", order == 9 ? 8 : order, dumpid, (long)nbody, tsys);
     std::fprintf(fp, "%A %A\n", init_energy, prev_energy);
     std::fprintf(fp, "%ld %ld\n", (long)steps, (long)block_steps);
-    for (int i = 0; i < nbody; ++i) {
+    bool ok = write_lines(fp, nbody, [&](int i, char *o) {
         const double *r = records + (size_t)i * R, *x = aux + (size_t)i * kAuxWords;
-        std::fprintf(fp, "%8ld %A", (long)(ids ? ids[i] : i), r[3]);
-        std::fprintf(fp, "   %A %A %A", r[0], r[1], r[2]);
-        if (order == 9)
-            std::fprintf(fp, "   %A %A %A", r[hb::kRecPosL], r[hb::kRecPosL + 1], r[hb::kRecPosL + 2]);
-        std::fprintf(fp, "   %A %A %A", r[4], r[5], r[6]);
-        for (int k = 8; k < Rd; k += 3) std::fprintf(fp, "   %A %A %A", r[k], r[k + 1], r[k + 2]);
-        std::fprintf(fp, "   %A %A %A", x[0], x[1], x[2]);
-        std::fprintf(fp, "   %A %A %A", x[3], x[4], x[5]);
-        std::fprintf(fp, "\n");
-    }
-    const bool ok = !std::ferror(fp);
+        char *const s = o;
+        o += put_id(ids ? ids[i] : i, 8, o);
+        *o++ = ' ';
+        o += put_hexA(r[3], o);
+        o += put_vec("   ", r, o);
+        if (order == 9) o += put_vec("   ", r + hb::kRecPosL, o);
+        o += put_vec("   ", r + 4, o);
+        for (int k = 8; k < Rd; k += 3) o += put_vec("   ", r + k, o);
+        o += put_vec("   ", x, o);
+        o += put_vec("   ", x + 3, o);
+        *o++ = '\n';
+        return (int)(o - s);
+    });
+    ok = ok && !std::ferror(fp);
     return (std::fclose(fp) == 0 && ok) ? HB_OK : HB_ERR_IO;
 }
 
@@ -135,34 +425,39 @@ int hb_dump_read(const char *path, int order, int nbody, long long *ids, double 
     if (!path || (order != 4 && order != 6 && order != 8 && order != 9) || nbody < 0 ||
         (nbody > 0 && (!records || !aux)))
         return HB_ERR_INVALID;
-    FILE *fp = std::fopen(path, "r");
-    if (!fp) return HB_ERR_IO;
-    int o = 0, d = 0;
-    long n = 0, st = 0, bs = 0;
+    Text buf;
+    if (!slurp(path, buf)) return HB_ERR_IO;
+    // header: order dumpid / nbody / tsys / two energies / two step counts
+    const char *p = buf.c_str();
+    long long o = 0, d = 0, n = 0, st = 0, bs = 0;
     double t = 0.0, e0 = 0.0, e1 = 0.0;
-    bool ok = std::fscanf(fp, "%d %d %ld %lf", &o, &d, &n, &t) == 4 &&
-              std::fscanf(fp, "%lA %lA", &e0, &e1) == 2 && std::fscanf(fp, "%ld %ld", &st, &bs) == 2 &&
-              o == (order == 9 ? 8 : order) && n == nbody;
+    const bool hdr = next_long(p, &o) && next_long(p, &d) && next_long(p, &n) && next_double(p, &t) &&
+                     next_double(p, &e0) && next_double(p, &e1) && next_long(p, &st) &&
+                     next_long(p, &bs);
+    if (!hdr || o != (order == 9 ? 8 : order) || n != nbody) return HB_ERR_IO;
+    // per particle: id, then mass, pos, [posL], vel, the record's derivatives
+    // and the two aux vectors, in file order
     const int R = 8 + 3 * (order - 2);
     const int Rd = order == 9 ? hb::kRecPosL : R;
-    for (int i = 0; ok && i < nbody; ++i) {
+    const int nv = 1 + 3 + (order == 9 ? 3 : 0) + 3 + (Rd - 8) + 6;
+    std::unique_ptr<double[]> vals(new double[(size_t)nbody * nv]);   // not zero-filled
+    std::vector<long long> idv(ids ? 0 : (size_t)nbody);
+    if (!parse_records(buf, (size_t)(p - buf.c_str()), nbody, nv, ids ? ids : idv.data(), vals.get()))
+        return HB_ERR_IO;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nbody; ++i) {
+        const double *v = vals.get() + (size_t)i * nv;
         double *r = records + (size_t)i * R, *x = aux + (size_t)i * kAuxWords;
-        long id = 0;
-        ok = std::fscanf(fp, "%ld %lA", &id, &r[3]) == 2 &&
-             std::fscanf(fp, "%lA %lA %lA", &r[0], &r[1], &r[2]) == 3;
-        if (ok && order == 9)
-            ok = std::fscanf(fp, "%lA %lA %lA", &r[hb::kRecPosL], &r[hb::kRecPosL + 1],
-                             &r[hb::kRecPosL + 2]) == 3;
-        ok = ok && std::fscanf(fp, "%lA %lA %lA", &r[4], &r[5], &r[6]) == 3;
+        r[3] = *v++;
+        for (int k = 0; k < 3; ++k) r[k] = *v++;
+        if (order == 9)
+            for (int k = 0; k < 3; ++k) r[hb::kRecPosL + k] = *v++;
+        for (int k = 4; k < 7; ++k) r[k] = *v++;
         r[7] = t;
-        for (int k = 8; ok && k < Rd; k += 3)
-            ok = std::fscanf(fp, "%lA %lA %lA", &r[k], &r[k + 1], &r[k + 2]) == 3;
-        ok = ok && std::fscanf(fp, "%lA %lA %lA", &x[0], &x[1], &x[2]) == 3 &&
-             std::fscanf(fp, "%lA %lA %lA", &x[3], &x[4], &x[5]) == 3;
-        if (ids) ids[i] = id;
+        for (int k = 8; k < Rd; ++k) r[k] = *v++;
+        for (int k = 0; k < kAuxWords; ++k) x[k] = *v++;
     }
-    std::fclose(fp);
-    return ok ? HB_OK : HB_ERR_IO;
+    return HB_OK;
 }
 
 }  // extern "C"
@@ -174,46 +469,6 @@ int hb_dump_read(const char *path, int order, int nbody, long long *ids, double 
 // %A" (id, mass, pos, vel, potential).  Large files are the start-up cost of
 // big runs, so both directions work on the whole file in memory and split the
 // particle lines over host threads.
-
-namespace {
-
-bool slurp(const char *path, std::string &buf)
-{
-    FILE *fp = std::fopen(path, "rb");
-    if (!fp) return false;
-    std::fseek(fp, 0, SEEK_END);
-    const long sz = std::ftell(fp);
-    std::fseek(fp, 0, SEEK_SET);
-    if (sz < 0) {
-        std::fclose(fp);
-        return false;
-    }
-    buf.resize((size_t)sz);
-    const size_t got = sz ? std::fread(&buf[0], 1, (size_t)sz, fp) : 0;
-    std::fclose(fp);
-    return got == (size_t)sz;
-}
-
-// Position after the header's three tokens; -1 if malformed.
-long parse_snap_header(const std::string &buf, int *snapid, long *n, double *t)
-{
-    const char *p = buf.c_str();
-    char *e = nullptr;
-    const long sid = std::strtol(p, &e, 10);
-    if (e == p) return -1;
-    p = e;
-    const long nb = std::strtol(p, &e, 10);
-    if (e == p || nb < 0) return -1;
-    p = e;
-    const double tt = std::strtod(p, &e);
-    if (e == p) return -1;
-    *snapid = (int)sid;
-    *n = nb;
-    *t = tt;
-    return (long)(e - buf.c_str());
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -238,41 +493,21 @@ int hb_snapshot_read(const char *path, int nbody, long long *ids, double *mass, 
                      double *vel, double *pot)
 {
     if (!path || nbody < 0 || (nbody > 0 && (!mass || !pos || !vel))) return HB_ERR_INVALID;
-    std::string buf;
+    Text buf;
     if (!slurp(path, buf)) return HB_ERR_IO;
-    int sid;
-    long n;
-    double t;
-    const long body = parse_snap_header(buf, &sid, &n, &t);
-    if (body < 0 || n != nbody) return HB_ERR_IO;
-    // line starts of the particle records
-    std::vector<long> start;
-    start.reserve((size_t)nbody + 1);
-    long p = body;
-    const long len = (long)buf.size();
-    while (p < len && (int)start.size() < nbody) {
-        while (p < len && (buf[p] == '\n' || buf[p] == '\r' || buf[p] == ' ' || buf[p] == '\t')) ++p;
-        if (p >= len) break;
-        start.push_back(p);
-        while (p < len && buf[p] != '\n') ++p;
-    }
-    if ((int)start.size() != nbody) return HB_ERR_IO;
-    int bad = 0;
-    const char *base = buf.c_str();
-#pragma omp parallel for schedule(static) reduction(| : bad)
+    const char *p = buf.c_str();
+    long long sid = 0, n = 0;
+    double t = 0.0;
+    if (!(next_long(p, &sid) && next_long(p, &n) && next_double(p, &t)) || n != nbody)
+        return HB_ERR_IO;
+    constexpr int nv = 8;   // mass, pos, vel, potential
+    std::unique_ptr<double[]> vals(new double[(size_t)nbody * nv]);   // not zero-filled
+    std::vector<long long> idv(ids ? 0 : (size_t)nbody);
+    if (!parse_records(buf, (size_t)(p - buf.c_str()), nbody, nv, ids ? ids : idv.data(), vals.get()))
+        return HB_ERR_IO;
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < nbody; ++i) {
-        const char *q = base + start[i];
-        char *e = nullptr;
-        const long long id = std::strtoll(q, &e, 10);
-        bad |= e == q;
-        q = e;
-        double v[8];
-        for (int k = 0; k < 8; ++k) {
-            v[k] = std::strtod(q, &e);
-            bad |= e == q;
-            q = e;
-        }
-        if (ids) ids[i] = id;
+        const double *v = vals.get() + (size_t)i * nv;
         mass[i] = v[0];
         for (int k = 0; k < 3; ++k) {
             pos[3 * (size_t)i + k] = v[1 + k];
@@ -280,7 +515,7 @@ int hb_snapshot_read(const char *path, int nbody, long long *ids, double *mass, 
         }
         if (pot) pot[i] = v[7];
     }
-    return bad ? HB_ERR_IO : HB_OK;
+    return HB_OK;
 }
 
 int hb_snapshot_write(const char *path, int snapid, int nbody, double tsys, const long long *ids,
@@ -290,24 +525,18 @@ int hb_snapshot_write(const char *path, int snapid, int nbody, double tsys, cons
     FILE *fp = std::fopen(path, "w");
     if (!fp) return HB_ERR_IO;
     std::fprintf(fp, "%d\n%ld\n%f\n", snapid, (long)nbody, tsys);
-    constexpr int kBlock = 4096;   // particles formatted per task
-    const int nblk = (nbody + kBlock - 1) / kBlock;
-    std::vector<std::string> out((size_t)nblk);
-#pragma omp parallel for schedule(dynamic)
-    for (int b = 0; b < nblk; ++b) {
-        std::string &s = out[b];
-        char line[512];
-        const int i1 = std::min(nbody, (b + 1) * kBlock);
-        for (int i = b * kBlock; i < i1; ++i) {
-            const double *x = pos + 3 * (size_t)i, *v = vel + 3 * (size_t)i;
-            const int m = std::snprintf(line, sizeof line, "%6ld    %A    %A %A %A    %A %A %A    %A\n",
-                                        (long)(ids ? ids[i] : i), mass[i], x[0], x[1], x[2], v[0],
-                                        v[1], v[2], pot ? pot[i] : 0.0);
-            s.append(line, (size_t)m);
-        }
-    }
-    bool ok = true;
-    for (const std::string &s : out) ok = ok && std::fwrite(s.data(), 1, s.size(), fp) == s.size();
+    bool ok = write_lines(fp, nbody, [&](int i, char *o) {
+        char *const s = o;
+        o += put_id(ids ? ids[i] : i, 6, o);
+        for (int k = 0; k < 4; ++k) *o++ = ' ';
+        o += put_hexA(mass[i], o);
+        o += put_vec("    ", pos + 3 * (size_t)i, o);
+        o += put_vec("    ", vel + 3 * (size_t)i, o);
+        for (int k = 0; k < 4; ++k) *o++ = ' ';
+        o += put_hexA(pot ? pot[i] : 0.0, o);
+        *o++ = '\n';
+        return (int)(o - s);
+    });
     ok = ok && !std::ferror(fp);
     return (std::fclose(fp) == 0 && ok) ? HB_OK : HB_ERR_IO;
 }
