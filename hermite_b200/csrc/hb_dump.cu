@@ -313,11 +313,9 @@ int put_hexA(double x, char *o)
 }
 
 // Formats lines [0, nbody) with line(i, out) -> bytes written (at most
-// kMaxLine), in blocks over host threads, and writes them in order.
-constexpr int kMaxLine = 2048;
-
+// max_line), in blocks over host threads, and writes them in order.
 template <typename LineFn>
-bool write_lines(FILE *fp, int nbody, LineFn line)
+bool write_lines(FILE *fp, int nbody, size_t max_line, LineFn line)
 {
     constexpr int kBlock = 4096;   // lines formatted per task
     const int nblk = (nbody + kBlock - 1) / kBlock;
@@ -326,7 +324,7 @@ bool write_lines(FILE *fp, int nbody, LineFn line)
 #pragma omp parallel for schedule(dynamic)
     for (int b = 0; b < nblk; ++b) {
         const int i0 = b * kBlock, i1 = std::min(nbody, i0 + kBlock);
-        out[b].reset(new char[(size_t)(i1 - i0) * kMaxLine]);
+        out[b].reset(new char[(size_t)(i1 - i0) * max_line]);
         char *o = out[b].get();
         size_t u = 0;
         for (int i = i0; i < i1; ++i) u += (size_t)line(i, o + u);
@@ -338,6 +336,9 @@ bool write_lines(FILE *fp, int nbody, LineFn line)
 }
 
 // "%<width>ld" of v.
+constexpr size_t kMaxHexA = 24;   // "-0X1.FFFFFFFFFFFFFP-1022"
+constexpr size_t kMaxId = 24;     // "%8lld" of any long long, with its NUL
+
 inline int put_id(long long v, int width, char *o)
 {
     return std::snprintf(o, 32, "%*lld", width, v);
@@ -374,7 +375,9 @@ int hb_dump_write(const char *path, int order, int dumpid, int nbody, double tsy
     std::fprintf(fp, "%d %d\n%ld\n%20.16f\n", order == 9 ? 8 : order, dumpid, (long)nbody, tsys);
     std::fprintf(fp, "%A %A\n", init_energy, prev_energy);
     std::fprintf(fp, "%ld %ld\n", (long)steps, (long)block_steps);
-    bool ok = write_lines(fp, nbody, [&](int i, char *o) {
+    const int ngroups = 2 + (order == 9 ? 1 : 0) + (Rd - 8) / 3 + 2;   // pos [posL] vel derivs aux
+    const size_t max_line = kMaxId + 1 + kMaxHexA + (size_t)ngroups * (3 + 3 * kMaxHexA + 2) + 1;
+    bool ok = write_lines(fp, nbody, max_line, [&](int i, char *o) {
         const double *r = records + (size_t)i * R, *x = aux + (size_t)i * kAuxWords;
         char *const s = o;
         o += put_id(ids ? ids[i] : i, 8, o);
@@ -525,7 +528,8 @@ int hb_snapshot_write(const char *path, int snapid, int nbody, double tsys, cons
     FILE *fp = std::fopen(path, "w");
     if (!fp) return HB_ERR_IO;
     std::fprintf(fp, "%d\n%ld\n%f\n", snapid, (long)nbody, tsys);
-    bool ok = write_lines(fp, nbody, [&](int i, char *o) {
+    const size_t max_line = kMaxId + 4 + kMaxHexA + 2 * (4 + 3 * kMaxHexA + 2) + 4 + kMaxHexA + 1;
+    bool ok = write_lines(fp, nbody, max_line, [&](int i, char *o) {
         char *const s = o;
         o += put_id(ids ? ids[i] : i, 6, o);
         for (int k = 0; k < 4; ++k) *o++ = ' ';
