@@ -212,6 +212,20 @@ def _dptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+def _out_buffer(out, rows: int, cols: int | None = None) -> np.ndarray:
+    """A caller's result array, checked before the library writes rows x
+    cols doubles into it (a new array when out is None)."""
+    shape = (max(int(rows), 0),) if cols is None else (max(int(rows), 0), int(cols))
+    if out is None:
+        return np.empty(shape, dtype=np.float64)
+    if not isinstance(out, np.ndarray) or out.dtype != np.float64 or not out.flags.c_contiguous \
+            or not out.flags.writeable:
+        raise ValueError("out must be a writeable C-contiguous float64 array")
+    if out.size < int(np.prod(shape)):
+        raise ValueError(f"out holds {out.size} doubles, {int(np.prod(shape))} needed")
+    return out
+
+
 def measure_fma_peak(mode: int) -> float:
     """Measured FMA-pipe peak in GFLOP/s: mode 0 FP64, 1 FP32, 2 packed FP32."""
     lib = load_library()
@@ -285,15 +299,13 @@ class Gravity:
         self._check(self._lib.hb_predict_all(self._h, float(tsys)), "predict_all")
 
     def calc_force_on_first_nact(self, nact: int, eps2: float, out: np.ndarray | None = None):
-        if out is None:
-            out = np.empty((max(int(nact), 0), self.F), dtype=np.float64)
+        out = _out_buffer(out, nact, self.F)
         self._check(self._lib.hb_force_first_nact(self._h, int(nact), float(eps2), _dptr(out)),
                     "calc_force_on_first_nact")
         return out
 
     def calc_potential(self, eps2: float, out: np.ndarray | None = None):
-        if out is None:
-            out = np.empty(self.nbody, dtype=np.float64)
+        out = _out_buffer(out, self.nbody)
         self._check(self._lib.hb_potential(self._h, float(eps2), _dptr(out)), "calc_potential")
         return out
 
@@ -320,8 +332,7 @@ class Gravity:
         self._check(self._lib.hb_force_device(self._h, int(nact), float(eps2)), "force_device")
 
     def download_forces(self, nact: int, out: np.ndarray | None = None):
-        if out is None:
-            out = np.empty((int(nact), self.F), dtype=np.float64)
+        out = _out_buffer(out, nact, self.F)
         self._check(self._lib.hb_download_forces(self._h, int(nact), _dptr(out)), "download_forces")
         return out
 

@@ -5,6 +5,7 @@ import ctypes
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 import hermite_b200 as hb
@@ -93,3 +94,20 @@ int main() { return sizeof(Gravity::GParticle) == 160 && sizeof(Gravity::GPredic
                            capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
         assert subprocess.run([str(Path(d) / "t")]).returncode == 0
+
+
+def test_result_buffers_are_checked():
+    """Caller-supplied result arrays are checked before the library writes
+    into them: dtype, layout, writeability and size."""
+    from hermite_b200 import _out_buffer
+    assert _out_buffer(None, 5, 6).shape == (5, 6) and _out_buffer(None, -1, 6).shape == (0, 6)
+    ok = np.empty((8, 6))
+    assert _out_buffer(ok, 5, 6) is ok
+    for bad in (np.empty((4, 6)), np.empty((5, 6), np.float32), np.empty((6, 10))[:, :6],
+                [[0.0] * 6] * 5):
+        with pytest.raises(ValueError):
+            _out_buffer(bad, 5, 6)
+    ro = np.empty(100)
+    ro.flags.writeable = False
+    with pytest.raises(ValueError):
+        _out_buffer(ro, 100)
