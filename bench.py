@@ -15,14 +15,14 @@ the reference's "Init N square" step, SRC/nbodysystem.h:582-594):
             memory (device->host), all inside the timed region.
 Extra keys: the roofline of the force kernel against the FP64 FMA peak
 measured in the same run; the reference's own AVX2 CPU Gravity (built from
-its sources into oracle/_ref/) on a bounded sample as cpu_baseline; the
-mixed-precision vs FP64 6th-order kernels at N = 262144 with their force
-errors (configs[2]-style); block-step latency through the C ABI at several
-nact.
+its sources into oracle/_ref/) on the same full step, repeated for at least
+10 s, as cpu_baseline; the mixed-precision vs FP64 6th-order kernels at
+N = 262144 with their force errors; block-step latency through the C ABI at
+several nact.
 
 --impl reference times the reference's AVX2 Gravity (set_jp, predict_all,
-calc_force_on_first_nact) on this host's cores, on a bounded sample of the
-same workload.  Under torchrun only rank 0 runs it.
+calc_force_on_first_nact) on this host's cores, on the same full step (K
+steps after W warm-up).  Under torchrun only rank 0 runs it.
 --gpus N > 1 runs N independent replicas (the path does not shard across
 GPUs in the reference; one process per GPU), timed as the max over ranks.
 """
@@ -167,8 +167,10 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
-def reference_force_rate(order, n, nact, reps, threads, rec=None):
-    """The reference's AVX2 Gravity (oracle/_ref) on this host: Gint/s."""
+def reference_force_rate(order, n, nact, threads, rec=None, min_s=10.0, min_reps=3, max_reps=200):
+    """The reference's AVX2 Gravity (oracle/_ref) on this host: Gint/s of
+    set_jp + predict_all + force on the first nact, repeated until min_s
+    seconds (at least min_reps, at most max_reps steps) after one warm-up."""
     from oracle import RefGravity
     os.environ["OMP_NUM_THREADS"] = str(threads)
     if rec is None:
@@ -179,7 +181,7 @@ def reference_force_rate(order, n, nact, reps, threads, rec=None):
     g.predict_all(0.0)
     g.force(nact, eps2)                     # warm-up
     times = []
-    for _ in range(reps):
+    while len(times) < max_reps and (len(times) < min_reps or sum(times) < min_s):
         t0 = time.perf_counter()
         g.set_jp_all(rec)
         g.predict_all(0.0)
@@ -200,7 +202,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/libref_avx4.so not built (needs the reference sources)"}))
         return
-    nact = 8192                              # bounded sample: 8192 i x 65536 j per step
+    nact = N                                 # the full step: all N i x N j
     rec = plummer_records(ORDER, N)
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from oracle import RefGravity
@@ -218,7 +220,8 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     g.close()
     value = nact * N * args.steps / dt * 1e-9
-    sample = f"force on the first {nact} of {N} particles from all {N} per step"
+    sample = (f"set_jp + predict_all + force on all {N} particles (the full step), "
+              f"{args.steps} steps after {args.warmup} warm-up")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
@@ -348,12 +351,11 @@ def run_ours(args):
             from oracle import ref_available
             if ref_available("avx", ORDER):
                 threads = host_threads()
-                nact = 8192
-                rate, times = reference_force_rate(ORDER, N, nact, 3, threads, rec)
+                rate, times = reference_force_rate(ORDER, N, N, threads, rec)
                 cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                        "sample": f"reference AVX2 Gravity (SRC/hermite4-avx.h, built from source): "
-                                 f"set_jp + predict_all + force on the first {nact} of {N} "
-                                 f"particles, 3 reps, {sum(times):.1f} s total"}
+                                 f"set_jp + predict_all + force on all {N} particles (the full "
+                                 f"step), {len(times)} steps, {sum(times):.1f} s total"}
         except Exception as e:          # the baseline is reported, not required
             cpu = {"value": None, "unit": UNIT, "cores": host_threads(), "kind": "reference",
                    "sample": f"failed: {e}"}
@@ -660,7 +662,7 @@ def small_ensemble_leg(nclusters=256, tend=1.0 / 16):
 
 
 def ensemble_leg(nclusters=256, tend=1.0 / 16, precision="fp64"):
-    """Batched ensemble (configs[4]-style): clusters with seeds 0..255, N
+    """Batched ensemble: 256 clusters with seeds 0..255, N
     log-uniform in [1024, 32768], power-law masses (slope -2.35 on [0.1, 100],
     total 1), eps = 4/N each, 6th order, eta = 0.1 (eta_s = eta/5),
     dtmax = 1/16, integrated by one device-resident loop; window

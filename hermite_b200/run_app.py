@@ -1,4 +1,4 @@
-"""Run the reference's own integrator on a BASELINE-style configuration.
+"""Run the reference's own integrator on one of the benchmark configurations.
 
 The integrator is the reference's SRC/compile.cpp + SRC/nbodysystem.h built
 unmodified against the drop-in Gravity (hermite_b200/gravity/_build/
