@@ -46,13 +46,15 @@ def test_close_to_reference_avx(order, oracle):
     np.testing.assert_allclose(oracle.potential(order, rec, EPS2), g.potential(EPS2), rtol=1e-14)
 
 
-@pytest.mark.parametrize("order", [4, 6, 8])
+@pytest.mark.parametrize("order", [4, 6, 8, 9])
 def test_golden_vectors(order, oracle):
     z = np.load(GOLDEN / f"ref_order{order}.npz")
     rec, nact, eps2 = z["records"], int(z["nact"]), float(z["eps2"])
     f = oracle.predict_force(order, rec, float(z["tsys"]), nact, eps2)
     assert np.array_equal(f, z["force"])
     assert np.array_equal(oracle.potential(order, rec, eps2), z["potential"])
+    if order == 9:          # double-double positions: the reference has no AVX backend
+        return
     assert rel_err(f, z["force_avx"]).max() < 1e-13
     np.testing.assert_allclose(oracle.potential(order, rec, eps2), z["potential_avx"], rtol=1e-14)
 
