@@ -9,6 +9,8 @@ derivatives suffer cancellation between pair terms and are bounded loosely
 here (jrk 1e-5, snp 1e-4, crk 1e-2 at these small N) -- their measured
 distributions are reported by bench.py.
 """
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -20,6 +22,7 @@ pytestmark = pytest.mark.gpu
 FP64_TOL = 1e-12
 MIXED_TOL = {0: 1e-6, 1: 1e-5, 2: 1e-4, 3: 1e-2}
 EPS2 = (1.0 / 256) ** 2
+GOLDEN = Path(__file__).resolve().parent / "golden"
 
 
 def _check(order, n, nact, precision, oracle, seed=1, eps2=EPS2, variant=-1, jsplit=0):
@@ -183,3 +186,19 @@ def test_predictor_pass_on_its_own(precision):
                 g.predict_pass()
             out.append(g.calc_force_on_first_nact(nact, EPS2))
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("order", [4, 6, 8, 9])
+def test_golden_fixtures(order):
+    """The reference's own outputs stored in tests/golden (its generic
+    Gravity, SRC/hermite{4,6,8}.h and SRC/hermite8dd.h, on 64 seeded slots):
+    the FP64 device force and potential match them to summation order."""
+    z = np.load(GOLDEN / f"ref_order{order}.npz")
+    rec, nact, eps2, tsys = z["records"], int(z["nact"]), float(z["eps2"]), float(z["tsys"])
+    with Gravity(8 if order == 9 else order, rec.shape[0], "dd" if order == 9 else "fp64") as g:
+        g.set_jp_records(rec)
+        g.predict_all(tsys)
+        got = g.calc_force_on_first_nact(nact, eps2)
+        pot = g.calc_potential(eps2)
+    assert rel_err(got, z["force"]).max() <= FP64_TOL
+    np.testing.assert_allclose(pot, z["potential"], rtol=1e-13, atol=0)
