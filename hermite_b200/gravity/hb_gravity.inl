@@ -87,4 +87,26 @@ struct Gravity {
     {
         check(ctx, hb_potential(ctx, eps2, potbuf), "calc_potential");
     }
+
+    // -DFAST_OMP_SYNC builds of the integrator call these from every thread of
+    // one OpenMP parallel region (SRC/nbodysystem.h:767-838), as the CPU
+    // backends provide them (SRC/hermite4-avx.h:9,155,404).  One thread drives
+    // the GPU; the integrator's barrier after the prediction, and the barrier
+    // here after the force, keep the others in step.  Above
+    // NACT_PARALLEL_THRESH active particles the integrator spreads set_jp over
+    // the threads, which set_jp allows for distinct slots.
+    enum { NACT_PARALLEL_THRESH = 8 };
+
+    void predict_all_fast_omp(const double tsys)
+    {
+#pragma omp master
+        predict_all(tsys);
+    }
+
+    void calc_force_on_first_nact_fast_omp(const int nact, const double eps2, Force force[])
+    {
+#pragma omp master
+        calc_force_on_first_nact(nact, eps2, force);
+#pragma omp barrier
+    }
 };

@@ -111,3 +111,21 @@ def test_result_buffers_are_checked():
     ro.flags.writeable = False
     with pytest.raises(ValueError):
         _out_buffer(ro, 100)
+
+
+@pytest.mark.parametrize("order", ["FOURTH", "SIXTH", "EIGHTH"])
+def test_fast_omp_sync_integrator_builds(order, tmp_path):
+    """The reference's -DFAST_OMP_SYNC integrator loop (one OpenMP region
+    per dtmax, SRC/nbodysystem.h:767-838) compiles and links against the
+    drop-in, which adds the members only its CPU backends had."""
+    import subprocess
+    gdir = ROOT / "hermite_b200" / "gravity"
+    ovl = gdir / "_build" / "overlay"
+    if not (ovl / "compile.cpp").exists() or not (gdir / "_build" / "parameter.o").exists():
+        pytest.skip("the reference integrator overlay is not built (needs the reference sources)")
+    r = subprocess.run(["g++", "-O1", "-fopenmp", "-w", "-I", str(ROOT / "include"), "-I", str(gdir),
+                        f"-D{order}", "-DCUDA_TITAN", "-DFAST_OMP_SYNC", "-I", str(ovl),
+                        str(ovl / "compile.cpp"), str(gdir / "_build" / "parameter.o"),
+                        "-L", str(ROOT / "hermite_b200" / "_lib"), "-lhermite_b200",
+                        "-o", str(tmp_path / "app")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
