@@ -9,7 +9,7 @@ reports are parsed:
   " de(local/global) : ..."                         (SRC/nbodysystem.h:948-951)
   "ke = .., pe = .., e = .."                        (SRC/nbodysystem.h:644-647)
 
-    python -m hermite_b200.run_app --config c1 [--impl gpu|gpu-mixed|cpu-ref|ref-gpu]
+    python -m hermite_b200.run_app --config c1 [--impl gpu|gpu-mixed|gpu-fast|cpu-ref|ref-gpu]
            [--tend T] [--n N]
 
 Configurations (Plummer spheres from hermite_b200.ic, seed 0, equal masses,
@@ -47,6 +47,8 @@ CONFIGS = {
 
 APP = {"gpu": ROOT / "hermite_b200" / "gravity" / "_build" / "hb-app-{order}",
        "gpu-mixed": ROOT / "hermite_b200" / "gravity" / "_build" / "hb-app-{order}",
+       # the integrator's -DFAST_OMP_SYNC loop on the drop-in (make -C hermite_b200/gravity fast)
+       "gpu-fast": ROOT / "hermite_b200" / "gravity" / "_build" / "hb-app-fast-{order}",
        "cpu-ref": ROOT / "oracle" / "_ref" / "avx2-{order}",
        # the reference's own FP64 CUDA path recompiled for sm_100a (oracle/Makefile ref-gpu)
        "ref-gpu": ROOT / "oracle" / "_ref" / "titan-{order}"}
