@@ -536,7 +536,7 @@ def ensemble_cpu_leg(nclusters=256, tend=1.0 / 16):
     interactions per second of each run and of the sample (the CPU
     counterpart of the ensemble's Gint/s)."""
     from hermite_b200.ic import plummer, power_law_masses
-    from hermite_b200.run_app import APP, run
+    from run_app import APP, run
     if not Path(str(APP["cpu-ref"]).format(order=6)).exists():
         return None
     rng = np.random.default_rng(2024)
@@ -588,7 +588,7 @@ def run_profile_case(case: str):
 def device_integrator_leg(configs=("c1", "c2")):
     """Block-step time of the device-resident integrator (corrector and
     scheduler on the GPU) on the plain-FP64 configurations c1 and c2 of
-    hermite_b200.run_app (eta = 0.01: the mixed path is not used at such
+    run_app.py (eta = 0.01: the mixed path is not used at such
     small eta, where FP32 force noise collapses the Aarseth steps): wall time
     per block step, particle steps x N / time, and the energy error.  c1
     (N = 1024) runs on both engines: "team" (one thread-block cluster, the
@@ -597,7 +597,7 @@ def device_integrator_leg(configs=("c1", "c2")):
     replay; the automatic choice for c2)."""
     from hermite_b200 import Gravity
     from hermite_b200.ic import plummer, records
-    from hermite_b200.run_app import CONFIGS
+    from run_app import CONFIGS
     out = {}
     for name in configs:
         cfg = dict(CONFIGS[name])
@@ -703,7 +703,7 @@ def reference_gpu_leg():
     headline workload: its own "## Init N square" report of one full N^2
     force evaluation at N = 65536, and its app-level block-step rate over a
     short window of configuration c2."""
-    from hermite_b200.run_app import APP, run
+    from run_app import APP, run
     if not Path(str(APP["ref-gpu"]).format(order=4)).exists():
         return None
     r = run("c2", "ref-gpu", tend=1.0 / 512)

@@ -1,10 +1,10 @@
 // hb_noalloc.cu -- force on predicted j-particles with no memory allocation.
 //
 // For callers that cannot call cudaMalloc: code embedded in a host framework
-// that owns every device allocation through its own pool, code that enqueues
-// work while a stream is being captured into a CUDA graph (where cudaMalloc is
-// not allowed), and fixed-budget jobs on a shared GPU that must not grow their
-// footprint after start-up.  They own the input and output buffers; the only
+// that owns every device allocation through its own pool (an allocation behind
+// the pool's back breaks its accounting or fails against its reservation),
+// and fixed-budget jobs on a shared GPU that must not grow their footprint
+// after start-up.  They own the input and output buffers; the only
 // scratch the force kernel needs (the j-slice partial sums and the per-i-tile
 // arrival counters) lives in the file-scope device array below, which the
 // library holds on every GPU it is loaded on until the process exits.
@@ -29,29 +29,32 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 struct DeviceScratch {
-    std::once_flag once;
-    cudaError_t status = cudaSuccess;
+    std::mutex mu;
     unsigned char *base = nullptr;   // device address of g_noalloc_scratch
     int nsm = 0;
 };
 DeviceScratch g_dev[kMaxDevices];
 
-// Once per device, with that device current: look up the device address of
-// the scratch array (its host-side name is only a stand-in) and the SM count.
+// With device `dev` current: the device address of the scratch array (its
+// host-side name is only a stand-in) and the SM count, looked up on the first
+// successful call for that device and kept from then on.  A failed lookup is
+// returned and not kept, so a later call tries again.
 cudaError_t scratch_for_device(int dev, DeviceScratch *&out)
 {
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     DeviceScratch &d = g_dev[dev];
-    std::call_once(d.once, [&d, dev]() {
+    std::lock_guard<std::mutex> lock(d.mu);
+    if (!d.base) {
         void *p = nullptr;
-        d.status = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (d.status == cudaSuccess) {
-            d.base = static_cast<unsigned char *>(p);
-            d.status = cudaDeviceGetAttribute(&d.nsm, cudaDevAttrMultiProcessorCount, dev);
-        }
-    });
+        int nsm = 0;
+        cudaError_t st = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (st == cudaSuccess) st = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (st != cudaSuccess) return st;
+        d.nsm = nsm;
+        d.base = static_cast<unsigned char *>(p);
+    }
     out = &d;
-    return d.status;
+    return cudaSuccess;
 }
 
 bool valid_order(int order) { return order == 4 || order == 6 || order == 8; }
@@ -96,7 +99,7 @@ extern "C" int hb_force_predicted_noalloc(int order, int precision, const void *
     // the i-tiles this launch uses must start at zero.
     if (S > 1 && cudaMemsetAsync(counter, 0, sizeof(unsigned) * gx, s) != cudaSuccess) return HB_ERR_CUDA;
 
-    hb::ForceArgs a;
+    hb::ForceArgs a{};
     a.pred = pred;
     a.nchunk = nchunk;
     a.nact = nact;
@@ -105,6 +108,11 @@ extern "C" int hb_force_predicted_noalloc(int order, int precision, const void *
     a.partial = reinterpret_cast<double *>(ds->base + kCounterBytes);
     a.counter = counter;
     a.err = nullptr;
-    fv->kern<<<dim3(gx, S), fv->nw * 32, fv->smem, s>>>(a);
-    return cudaGetLastError() == cudaSuccess ? HB_OK : HB_ERR_CUDA;
+    // cudaLaunchKernel returns this launch's own status, so an earlier,
+    // unrelated error on the caller's thread is neither blamed on this call
+    // nor cleared by it.
+    void *args[] = {&a};
+    const cudaError_t st = cudaLaunchKernel(reinterpret_cast<const void *>(fv->kern), dim3(gx, S),
+                                            dim3(fv->nw * 32), args, (size_t)fv->smem, s);
+    return st == cudaSuccess ? HB_OK : HB_ERR_CUDA;
 }

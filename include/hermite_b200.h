@@ -309,11 +309,10 @@ int hb_measure_fma_peak(int precision, double *gflops);
 /* ---- allocation-free force ---------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * code inside a host framework that owns every device allocation through its
- * own pool, code that enqueues work while a stream is being captured into a
- * CUDA graph (cudaMalloc is not allowed there), and fixed-budget jobs on a
- * shared GPU that must not grow their footprint after start-up.  hb_create
- * allocates, so such callers use this context-free entry point instead; it
- * allocates nothing.
+ * own pool (an allocation behind the pool's back breaks its accounting or
+ * fails against its reservation), and fixed-budget jobs on a shared GPU that
+ * must not grow their footprint after start-up.  hb_create allocates, so such
+ * callers use this context-free entry point instead; it allocates nothing.
  *
  * Computes the force on slots [0,nact) from all nslots slots, like
  * hb_force_device, from predicted j-particles the caller already holds in
@@ -330,9 +329,11 @@ int hb_measure_fma_peak(int precision, double *gflops);
  * beyond); larger nact get fewer j-slices, never a larger buffer.
  * Scratch: one file-scope device array of 4.125 MiB (4 MiB of j-slice
  * partial sums, 128 KiB of arrival counters) that every GPU loading the
- * library holds until the process exits.  The first call on each device looks
- * up that array's device address; make that first call before any stream
- * capture.  Every call shares the array and clears the counters it uses on
+ * library holds until the process exits.  The first call on each device (with
+ * that device current) looks up that array's device address; make that first
+ * call before any stream capture.  A lookup that fails returns HB_ERR_CUDA and
+ * is tried again by the next call.  Every call shares the array and clears
+ * the counters it uses on
  * its stream first; calls that overlap on the GPU (on different streams or
  * devices sharing a context) race on it and must be serialised by the caller.
  * A device-side wait that gives up is not reported by this entry point. */

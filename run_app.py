@@ -9,7 +9,7 @@ reports are parsed:
   " de(local/global) : ..."                         (SRC/nbodysystem.h:948-951)
   "ke = .., pe = .., e = .."                        (SRC/nbodysystem.h:644-647)
 
-    python -m hermite_b200.run_app --config c1 [--impl gpu|gpu-mixed|gpu-fast|cpu-ref|ref-gpu]
+    python run_app.py --config c1 [--impl gpu|gpu-mixed|gpu-fast|cpu-ref|ref-gpu]
            [--tend T] [--n N]
 
 Configurations (Plummer spheres from hermite_b200.ic, seed 0, equal masses,
@@ -33,7 +33,7 @@ import tempfile
 import time
 from pathlib import Path
 
-ROOT = Path(__file__).resolve().parent.parent
+ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 CONFIGS = {

@@ -1,8 +1,9 @@
 """The allocation-free force entry point, hb_force_predicted_noalloc.
 
 It serves callers that cannot call cudaMalloc: code inside a host framework
-that owns all device memory through its own pool, code enqueuing work while a
-stream is captured into a CUDA graph, and fixed-budget jobs on a shared GPU.
+that owns all device memory through its own pool (an allocation behind the
+pool's back breaks its accounting or fails against its reservation), and
+fixed-budget jobs on a shared GPU that must not grow their footprint.
 They pass their own device buffers (predicted j-particles in, forces out) and
 the entry point uses only its own static device scratch.
 
@@ -99,3 +100,37 @@ def test_noalloc_matches_context_path(order, precision, oracle):
             tol = FP64_TOL if precision == "fp64" else MIXED_TOL[k]
             assert err[:, k].max() <= tol, (order, precision, nact, k, err[:, k].max())
     assert np.array_equal(first, again)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order,n,nacts", [
+    # 8th order, nact 16384: the j-split wanted for occupancy (5 slices) needs
+    # more than the 4 MiB of partials, so the call takes fewer slices
+    (8, 65536, (16384, 5000)),
+    # 4th order, nact = N = 2^18: enough i-tiles to fill the GPU, one slice
+    # (no partials, no counters), then a split call after it
+    (4, 262144, (262144, 64)),
+])
+def test_noalloc_large_shapes(order, n, nacts, oracle):
+    import torch
+    lib = hb.load_library()
+    nslots = n
+    rec = make_records(order, n, seed=7 + order)
+    pred = oracle.predict(order, rec, 0.0)
+    d_pred = torch.from_numpy(pack_predicted(order, "fp64", pred, nslots)).cuda()
+    F = hb.force_words(order)
+    stream = torch.cuda.current_stream().cuda_stream
+    with hb.Gravity(order, n, "fp64") as g:
+        g.set_jp_records(rec)
+        g.predict_all(0.0)
+        ref = {nact: g.calc_force_on_first_nact(nact, EPS2) for nact in nacts}
+    for nact in nacts:          # two calls in a row on the shared scratch
+        out = torch.full((nact, F), float("nan"), dtype=torch.float64, device="cuda")
+        st = lib.hb_force_predicted_noalloc(order, hb.FP64, ctypes.c_void_p(d_pred.data_ptr()),
+                                            nslots, nact, EPS2, ctypes.c_void_p(out.data_ptr()),
+                                            ctypes.c_void_p(stream))
+        assert st == 0, lib.hb_status_string(st)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert np.all(np.isfinite(got))
+        assert rel_err(got, ref[nact]).max() <= FP64_TOL, (order, nact)
