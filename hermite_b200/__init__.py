@@ -44,7 +44,8 @@ EXPORTED_SYMBOLS = (
     "hb_force_first_nact", "hb_potential", "hb_set_precision", "hb_get_precision",
     "hb_last_error", "hb_status_string", "hb_set_stream", "hb_upload",
     "hb_predict_all_device", "hb_predict_pass", "hb_force_device", "hb_download_forces", "hb_device_forces",
-    "hb_synchronize", "hb_launch_count", "hb_set_force_shape", "hb_force_variant_count",
+    "hb_synchronize", "hb_launch_count", "hb_set_force_shape", "hb_set_wait_limit",
+    "hb_force_variant_count",
     "hb_force_variant_info", "hb_measure_fma_peak", "hb_force_predicted_noalloc",
     "hb_integrator_init", "hb_integrator_run", "hb_integrator_stats", "hb_energy",
     "hb_integrator_set_engine", "hb_integrator_engine",
@@ -158,6 +159,7 @@ def load_library() -> ctypes.CDLL:
         "hb_synchronize": (I, [P]),
         "hb_launch_count": (ctypes.c_longlong, [P]),
         "hb_set_force_shape": (I, [P, I, I]),
+        "hb_set_wait_limit": (I, [P, ctypes.c_longlong]),
         "hb_force_variant_count": (I, [I, I]),
         "hb_force_variant_info": (I, [I, I, I, ctypes.POINTER(I), ctypes.POINTER(I),
                                       ctypes.POINTER(I)]),
@@ -345,6 +347,12 @@ class Gravity:
     def set_force_shape(self, variant: int = -1, jsplit: int = 0):
         self._check(self._lib.hb_set_force_shape(self._h, int(variant), int(jsplit)),
                     "set_force_shape")
+
+
+    def set_wait_limit(self, polls: int = -1):
+        """Test hook: poll limit of the force kernel's waits for incoming j
+        tiles (0: give up at once; < 0: the default)."""
+        self._check(self._lib.hb_set_wait_limit(self._h, int(polls)), "set_wait_limit")
 
     def device_forces_ptr(self) -> int:
         return int(self._lib.hb_device_forces(self._h) or 0)

@@ -73,6 +73,7 @@ struct hb_ctx {
     int njpsend = 0;                // the reference's bookkeeping (previous nact)
     long long launches = 0;
     int variant_override = -1, jsplit_override = 0;
+    unsigned wait_limit = kSpinLimit;   // force kernel's tile waits (hb_set_wait_limit)
 
     // device-resident integration (hb_integrator_*)
     Sched *h_sched = nullptr;       // host copy of the scheduler (set-up only)
@@ -288,7 +289,7 @@ int run_force(hb_ctx *ctx, int nact, double eps2, double *force_out_dev)
         ctx->launches++;
         ctx->pred_stale = false;
     }
-    ForceArgs a;
+    ForceArgs a{};
     a.pred = ctx->d_pred;
     a.jp = ctx->d_jp;
     a.tsys = ctx->tsys;
@@ -300,6 +301,7 @@ int run_force(hb_ctx *ctx, int nact, double eps2, double *force_out_dev)
     a.partial = ctx->d_partial;
     a.counter = ctx->d_counter;
     a.err = ctx->d_err;
+    a.spin = ctx->wait_limit;
     fv->kern<<<dim3(gx, S), threads, fv->smem, ctx->stream>>>(a);
     HB_CK(cudaGetLastError());
     ctx->launches++;
@@ -639,6 +641,14 @@ int hb_set_force_shape(hb_ctx *ctx, int variant, int jsplit)
         return fail(ctx, HB_ERR_INVALID, "variant %d / jsplit %d out of range", variant, jsplit);
     ctx->variant_override = variant;   // < 0: automatic
     ctx->jsplit_override = jsplit;     // 0: automatic
+    return HB_OK;
+}
+
+int hb_set_wait_limit(hb_ctx *ctx, long long polls)
+{
+    if (!ctx) return HB_ERR_INVALID;
+    ctx->wait_limit = polls < 0 ? kSpinLimit
+                                : (unsigned)std::min<long long>(polls, (long long)kSpinLimit);
     return HB_OK;
 }
 

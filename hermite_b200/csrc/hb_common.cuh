@@ -114,11 +114,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return done != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`.  Returns false after kSpinLimit
-// polls (each try_wait itself suspends for a hardware-chosen time).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+// Bounded wait for phase `parity` of `bar`.  Returns false after `limit`
+// polls (each try_wait itself suspends for a hardware-chosen time).  Waits
+// that drain copies still in flight always take the full kSpinLimit.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint32_t limit = kSpinLimit)
 {
-    for (uint32_t it = 0; it < kSpinLimit; ++it)
+    for (uint32_t it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

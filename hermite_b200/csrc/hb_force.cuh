@@ -268,7 +268,7 @@ force_kernel(ForceArgs a)
             mbar_arrive_expect_tx(&bar[STG], bytes);
             bulk_load(smem, a.jp + (size_t)blockIdx.x * TI * Rec<ORDER>::words, bytes, &bar[STG]);
         }
-        const bool got = mbar_wait_bounded(&bar[STG], 0);
+        const bool got = mbar_wait_bounded(&bar[STG], 0, a.spin);
         if (!__syncthreads_and(got)) {
             if (tid == 0) {
                 raise_error(a.err, kErrWaitTimeout);
@@ -316,7 +316,7 @@ force_kernel(ForceArgs a)
     int failed_at = -1;
     for (int t = 0; t < ntile; ++t) {
         const int st = t % STG;
-        const bool got = mbar_wait_bounded(&bar[st], (uint32_t)((t / STG) & 1));
+        const bool got = mbar_wait_bounded(&bar[st], (uint32_t)((t / STG) & 1), a.spin);
         if (!__syncthreads_and(got)) { failed_at = t; break; }
         const int cnt = min(TCH, c1 - (c0 + t * TCH));
         const unsigned char *tile = smem + st * Sh::tile_bytes;

@@ -13,6 +13,8 @@ struct ForceArgs {
     double *partial;       // [S][gridDim.x*TI][F]  (only when S > 1)
     unsigned *counter;     // [gridDim.x], zero between launches
     int *err;              // mapped host flag
+    unsigned spin;         // poll limit of the waits for incoming tiles
+                           // (kSpinLimit; lowered only by hb_set_wait_limit)
     // fused predict + force only: raw j-particle records and the time to
     // predict them to (slots >= nbody are padding)
     const double *jp;

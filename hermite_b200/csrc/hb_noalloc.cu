@@ -108,6 +108,7 @@ extern "C" int hb_force_predicted_noalloc(int order, int precision, const void *
     a.partial = reinterpret_cast<double *>(ds->base + kCounterBytes);
     a.counter = counter;
     a.err = nullptr;
+    a.spin = hb::kSpinLimit;
     // cudaLaunchKernel returns this launch's own status, so an earlier,
     // unrelated error on the caller's thread is neither blamed on this call
     // nor cleared by it.

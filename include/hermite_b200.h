@@ -144,6 +144,16 @@ int hb_synchronize(hb_ctx *ctx);
 /* Number of kernels this context has launched so far. */
 long long hb_launch_count(const hb_ctx *ctx);
 
+/* Test hook: the poll limit of the force kernel's waits for incoming j tiles
+ * (default and maximum 1<<22 polls; polls < 0 restores the default).  A
+ * limit of 0 makes every such wait give up at once, so a test can drive the
+ * kernel's timeout path with no fault: the kernel raises its error flag, its
+ * waits for the copies already in flight keep the full limit, the call
+ * returns HB_ERR_DEVICE_TIMEOUT and the context stays usable.  No
+ * counterpart in the reference, whose CUDA path only aborts on errors
+ * (SRC/cuda_pointer.h:6-10). */
+int hb_set_wait_limit(hb_ctx *ctx, long long polls);
+
 /* Launch shape of the force kernel, picked per (order, precision, nbody,
  * nact) by the built-in tuning table unless overridden here.  variant
  * indexes the compiled kernel variants (see hb_force_variant_count);

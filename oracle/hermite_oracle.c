@@ -106,12 +106,15 @@ static inline double dot3(const double *a, const double *b)
  *   4th: SRC/hermite4.h:342-357  (acc, jerk)
  *   6th: SRC/hermite6.h:332-360  (+ snap; alpha, beta)
  *   8th: SRC/hermite8.h:385-425  (+ crackle; gamma)
- * j is summed in ascending order in FP64.
+ * j is summed in ascending order in FP64.  The i-particles are shared out
+ * over OpenMP threads (when built with -fopenmp); each i's sum stays a
+ * single ascending loop, so the result does not depend on the thread count.
  */
 void oracle_force(int order, int n, const double *pred, int nact, double eps2,
                   double *force)
 {
     const int P = pred_words(order), F = force_words(order);
+#pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < nact; i++) {
         const double *pi = pred + (size_t)i * P;
         double f[12] = {0};
@@ -174,6 +177,7 @@ void oracle_potential(int order, int n, const double *rec, double eps2,
                       double *pot)
 {
     const int R = rec_words(order);
+#pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < n; i++) {
         const double *pi = rec + (size_t)i * R;
         double s = 0.0;

@@ -51,10 +51,22 @@ def make_snapshot(workdir: Path, nk: int) -> str:
 
 def run_app(app: Path, order: int, nk: int, workdir: Path, env=None, timeout=600):
     """Run an integrator binary; return (nact strings, stdout)."""
+    nact, r = run_app_full(app, order, nk, workdir, env, timeout)
+    return nact, r.stdout
+
+
+def run_app_full(app: Path, order: int, nk: int, workdir: Path, env=None, timeout=600):
+    """Run an integrator binary; return (nact strings, the CompletedProcess)."""
     snap = make_snapshot(workdir, nk)
     r = subprocess.run([str(app)], input=input_text(order, snap), cwd=workdir, env=env,
                        capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"{app.name} failed ({r.returncode}):\n{r.stderr[-2000:]}")
     rows = re.findall(r"^## (\d+) (\S+) (\S+) (\S+) (\S+)\s*$", r.stdout, re.M)
-    return [row[4] for row in rows], r.stdout
+    return [row[4] for row in rows], r
+
+
+def energy_error(stderr: str) -> float:
+    """The last global relative energy error the integrator printed
+    (" de(local/global) : ..", SRC/nbodysystem.h:948-951)."""
+    return float(re.findall(r"de\(local/global\) : \S+ (\S+)", stderr)[-1])

@@ -1,0 +1,109 @@
+"""How much force error the reference's Hermite integrator tolerates, and why
+the mixed-precision pair arithmetic exceeds it at small eta and at 6th order.
+
+The reference's own integrator (SRC/nbodysystem.h with the corrector and
+Aarseth criterion of SRC/hermite{4,6}.h) runs on the CPU against
+tests/noise/noise_gravity.inl: the oracle's FP64 forces, optionally with a
+seeded relative perturbation of size s per derivative, or the mixed kernel's
+pair arithmetic restated in C float.  The corrector forms the higher
+derivatives from differences of consecutive forces of a particle, scaled by
+dt^-2..dt^-3 (4th order, SRC/hermite4.h:118-153) or dt^-3..dt^-5 (6th order,
+SRC/hermite6.h:136-184); white force noise of relative size s thus enters
+the step criterion amplified by about (tau/dt)^3 or (tau/dt)^5, and once it
+dominates, shorter steps amplify it further and the block steps collapse.
+
+Measured (block steps to t = 1/8, gen-plum-like Plummer N = 1024, eps = 1/256;
+6th order: N = 4096, eps = 1/4096, eta = 0.1, dtmax = 1/32, t = 1/32):
+  4th order, eta = 0.01: FP64 and s = 1e-9 take the same steps; s = 1e-8 and
+    the FP32 pair arithmetic blow up (> 10x), and so does FP64 arithmetic
+    whose relative position alone is the hi/lo FP32 difference: one FP32
+    rounding per pair already exceeds what the criterion tolerates.
+  4th order, eta = 0.1 (the reference's RUN/inp.4th): s = 1e-6 and the FP32
+    pair arithmetic take FP64's steps within 1%.
+  6th order, eta = 0.1: s = 1e-11 is tolerated, s = 1e-10 is not.
+FP32 pair arithmetic leaves s ~ 1e-8..1e-7 (tests/test_config_parity.py), so
+6th/8th-order integrations and 4th-order ones at eta of about 0.02 or less
+need the FP64 force; the mixed kernel integrates 4th order at the
+reference's own eta.
+"""
+import os
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+NOISE = ROOT / "tests" / "noise"
+BLOWUP = 3            # noise_gravity's exit code when HB_NOISE_MAX_CALLS is reached
+
+
+@pytest.fixture(scope="module")
+def apps():
+    sys.path.insert(0, str(ROOT))
+    from __graft_entry__ import reference_checkout
+    ref = reference_checkout()
+    if ref is None:
+        pytest.skip("the reference checkout is needed to build its integrator")
+    r = subprocess.run(["make", "-C", str(NOISE), f"REF={ref}"], capture_output=True, text=True)
+    if r.returncode != 0:
+        pytest.fail(f"building tests/noise failed:\n{r.stderr[-2000:]}")
+    return NOISE / "_build"
+
+
+def run(apps, tmp_path, order, n, eps, eta, eta_s, dtmax_inv, tend, env, max_calls=0):
+    """Block steps and energy error of one run (None when it blew up)."""
+    from hermite_b200.ic import plummer, write_snapshot
+    snap = tmp_path / f"plummer_{n}.dat"
+    if not snap.exists():
+        write_snapshot(snap, plummer(n, 0))
+    text = (f"order {order}\neta {eta!r}\neta_s {eta_s!r}\nsnapin {snap.name}\n"
+            f"tend {tend!r}\ndtmaxinv {dtmax_inv}\neps {eps!r}\nlog_interval {tend!r}\n"
+            f"snap_interval {2 * tend!r}\ndump_interval {tend!r}\n")
+    e = dict(os.environ, OMP_NUM_THREADS=str(min(8, os.cpu_count() or 1)))
+    e.update({k: str(v) for k, v in env.items()})
+    if max_calls:
+        e["HB_NOISE_MAX_CALLS"] = str(max_calls)
+    r = subprocess.run([str(apps / f"noise-app-{order}")], input=text, cwd=tmp_path, env=e,
+                       capture_output=True, text=True, timeout=600)
+    if r.returncode == BLOWUP or "Assertion `dtlim" in r.stderr:
+        return None
+    assert r.returncode == 0, r.stderr[-2000:]
+    steps = re.findall(r"steps: (\d+) (\d+) (\d+) (\d+)", r.stderr)
+    de = re.findall(r"de\(local/global\) : (\S+) (\S+)", r.stderr)
+    return int(steps[-1][2]), float(de[-1][1])
+
+
+C1 = dict(order=4, n=1024, eps=1 / 256, dtmax_inv=8, tend=0.125)
+C3S = dict(order=6, n=4096, eps=1 / 4096, eta=0.1, eta_s=0.02, dtmax_inv=32, tend=1 / 32)
+
+
+def test_fourth_order_small_eta(apps, tmp_path):
+    c1 = dict(C1, eta=0.01, eta_s=0.0025)
+    bs64, de64 = run(apps, tmp_path, env={}, **c1)
+    cap = 10 * bs64
+    quiet = run(apps, tmp_path, env={"HB_NOISE_REL": 1e-9}, max_calls=cap, **c1)
+    assert quiet is not None and quiet[0] <= 1.1 * bs64
+    assert run(apps, tmp_path, env={"HB_NOISE_REL": 1e-8}, max_calls=cap, **c1) is None
+    assert run(apps, tmp_path, env={"HB_NOISE_MODE": "fp32pair"}, max_calls=cap, **c1) is None
+    # one FP32 rounding per pair, of the relative position, is enough
+    assert run(apps, tmp_path, env={"HB_NOISE_MODE": "dr32"}, max_calls=cap, **c1) is None
+
+
+def test_fourth_order_reference_eta(apps, tmp_path):
+    c1 = dict(C1, eta=0.1, eta_s=0.01)
+    bs64, de64 = run(apps, tmp_path, env={}, **c1)
+    for env in ({"HB_NOISE_REL": 1e-6}, {"HB_NOISE_MODE": "fp32pair"}):
+        bs, de = run(apps, tmp_path, env=env, max_calls=10 * bs64, **c1)
+        assert abs(bs - bs64) <= 0.01 * bs64, (env, bs, bs64)
+        assert abs(de) <= 2 * abs(de64) + 1e-12, (env, de, de64)
+
+
+def test_sixth_order(apps, tmp_path):
+    bs64, de64 = run(apps, tmp_path, env={}, **C3S)
+    cap = 10 * bs64
+    quiet = run(apps, tmp_path, env={"HB_NOISE_REL": 1e-11}, max_calls=cap, **C3S)
+    assert quiet is not None and quiet[0] <= 1.1 * bs64
+    assert run(apps, tmp_path, env={"HB_NOISE_REL": 1e-10}, max_calls=cap, **C3S) is None
+    assert run(apps, tmp_path, env={"HB_NOISE_MODE": "fp32pair"}, max_calls=cap, **C3S) is None
