@@ -2,27 +2,32 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Headline workload (one "step" = one block step with every particle active,
-the reference's "Init N square" step, SRC/nbodysystem.h:582-594):
-    plain FP64 4th order, Plummer N = 65536, equal masses, Henon units,
-    eps = 1/1024: predict_all over all N, then the force on all N (N^2
-    interactions, self pair included, 60 flops each by the reference's
-    convention, SRC/hermite4.h:19).
+Headline workload: the 6th-order configuration of the metric -- Plummer
+N = 262144, equal masses, Henon units, eps = 1/4096 -- in plain FP64, the
+reference's own precision.  One "step" is one block step with every particle
+active, the reference's "Init N square" step (SRC/nbodysystem.h:582-594):
+predict_all over all N, then the force on all N (N^2 interactions, self pair
+included, 97 flops each by the reference's convention, SRC/hermite6.h:22).
   value  -- Gint/s with inputs resident in HBM (predictor + force kernels),
             L2 flushed before every timed step.
   e2e    -- the same step through the C ABI with host buffers: set_jp of
             all N records, predict_all (host->device upload), force into host
             memory (device->host), all inside the timed region.
+  mixed  -- the same step with the mixed-precision force kernel, its rate
+            against the FP64 kernel's, and both precisions' force errors
+            against the FP64 oracle on integrator states (4096 sampled i
+            against all N).
 Extra keys: the roofline of the force kernel against the FP64 FMA peak
 measured in the same run; the reference's own AVX2 CPU Gravity (built from
-its sources into oracle/_ref/) on the same full step, repeated for at least
-10 s, as cpu_baseline; the mixed-precision vs FP64 6th-order kernels at
-N = 262144 with their force errors; block-step latency through the C ABI at
-several nact.
+its sources into oracle/_ref/) on a sample of the same step (set_jp and
+predict_all of all N, the force on the first 8192 i against all N), repeated
+for at least 10 s, as cpu_baseline; block-step times of the device-resident
+integrator; the 8th-order configuration; batched ensembles; the force noise
+of the mixed kernel against what the step criterion tolerates.
 
 --impl reference times the reference's AVX2 Gravity (set_jp, predict_all,
-calc_force_on_first_nact) on this host's cores, on the same full step (K
-steps after W warm-up).  Under torchrun only rank 0 runs it.
+calc_force_on_first_nact) on this host's cores on the same sample of the
+step (K steps after W warm-up).  Under torchrun only rank 0 runs it.
 --gpus N > 1 runs N independent replicas (the path does not shard across
 GPUs in the reference; one process per GPU), timed as the max over ranks.
 """
@@ -45,13 +50,15 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Gint/s & block-step time, mixed-prec vs FP64 kernel, 1 B200, at stated force/energy err"
 UNIT = "Gint/s"
-ORDER, N, EPS = 4, 65536, 1.0 / 1024
+ORDER, N, EPS = 6, 262144, 1.0 / 4096
+CPU_NACT = 8192            # i-particles of the CPU sample of the step
+NSAMPLE = 4096             # i-particles of the accuracy sample
 FLOPS = {4: 60, 6: 97, 8: 144}
 L2_FLUSH_BYTES = 256 << 20
 
 
 def workload_config(extra=None):
-    cfg = {"workload": "Plummer N=65536 equal-mass Henon units, eps=1/1024, 4th-order Hermite, "
+    cfg = {"workload": "Plummer N=262144 equal-mass Henon units, eps=1/4096, 6th-order Hermite, "
                        "plain FP64; one step = predict_all + force on all N (full block step)",
            "order": ORDER, "nbody": N, "nact": N, "eps": EPS, "precision": "fp64",
            "flops_per_interaction": FLOPS[ORDER], "l2": "flushed (256 MiB write) before each step",
@@ -169,8 +176,9 @@ def host_threads() -> int:
 
 def reference_force_rate(order, n, nact, threads, rec=None, min_s=10.0, min_reps=3, max_reps=200):
     """The reference's AVX2 Gravity (oracle/_ref) on this host: Gint/s of
-    set_jp + predict_all + force on the first nact, repeated until min_s
-    seconds (at least min_reps, at most max_reps steps) after one warm-up."""
+    set_jp of all n + predict_all + force on the first nact against all n,
+    repeated until min_s seconds (at least min_reps, at most max_reps steps)
+    after one warm-up."""
     from oracle import RefGravity
     os.environ["OMP_NUM_THREADS"] = str(threads)
     if rec is None:
@@ -191,6 +199,11 @@ def reference_force_rate(order, n, nact, threads, rec=None, min_s=10.0, min_reps
     return nact * n / (sum(times) / len(times)) * 1e-9, times
 
 
+def cpu_sample_text(steps, extra=""):
+    return (f"set_jp + predict_all of all {N} particles, force on the first {CPU_NACT} i "
+            f"against all {N} j ({CPU_NACT * N:.3g} interactions per step), {steps} steps{extra}")
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -200,9 +213,8 @@ def run_reference(args):
     from oracle import ref_available
     if not ref_available("avx", ORDER):
         print(json.dumps({"impl": "reference", "unavailable":
-                          "oracle/_ref/libref_avx4.so not built (needs the reference sources)"}))
+                          f"oracle/_ref/libref_avx{ORDER}.so not built (needs the reference sources)"}))
         return
-    nact = N                                 # the full step: all N i x N j
     rec = plummer_records(ORDER, N)
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from oracle import RefGravity
@@ -211,23 +223,23 @@ def run_reference(args):
     for _ in range(args.warmup):
         g.set_jp_all(rec)
         g.predict_all(0.0)
-        g.force(nact, eps2)
+        g.force(CPU_NACT, eps2)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         g.set_jp_all(rec)
         g.predict_all(0.0)
-        g.force(nact, eps2)
+        g.force(CPU_NACT, eps2)
     dt = time.perf_counter() - t0
     g.close()
-    value = nact * N * args.steps / dt * 1e-9
-    sample = (f"set_jp + predict_all + force on all {N} particles (the full step), "
-              f"{args.steps} steps after {args.warmup} warm-up")
+    value = CPU_NACT * N * args.steps / dt * 1e-9
+    sample = cpu_sample_text(args.steps, f" after {args.warmup} warm-up")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config({"impl": "reference AVX2 Gravity "
-                                                        "(SRC/hermite4-avx.h) on host cores"}),
+                                                        "(SRC/hermite6-avx.h) on host cores",
+                                                        "nact_sampled": CPU_NACT}),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -235,9 +247,9 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
-def traffic_from_profiles():
-    """dram bytes per force-kernel launch from the committed ncu summary."""
-    p = ROOT / "profiles" / "force_fp64_o4_n65536.txt"
+def traffic_from_profiles(name):
+    """dram bytes per force-kernel launch from a committed ncu summary."""
+    p = ROOT / "profiles" / name
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
@@ -247,6 +259,25 @@ def traffic_from_profiles():
             except ValueError:
                 return None
     return None
+
+
+def timed_steps(g, stream, flush, steps, eps2, t0=0.0):
+    """CUDA-event times (ms) of `steps` device-resident steps: L2 flush,
+    predict_all to a new time, force on all N."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        e0, e1, e2 = ev[k]
+        e0.record(stream)
+        g.predict_all_device(t0 + 1e-6 * (k + 1))
+        e1.record(stream)
+        g.force_device(N, eps2)
+        e2.record(stream)
+    stream.synchronize()
+    return ([a.elapsed_time(c) for a, b, c in ev], [a.elapsed_time(b) for a, b, c in ev],
+            [b.elapsed_time(c) for a, b, c in ev])
 
 
 def run_ours(args):
@@ -261,6 +292,7 @@ def run_ours(args):
     rec = plummer_records(ORDER, N, seed=rank)
     eps2 = EPS * EPS
     nint = float(N) * N
+    F = 3 * (ORDER // 2)
 
     with torch.cuda.stream(stream):
         g = Gravity(ORDER, N, "fp64")
@@ -273,31 +305,19 @@ def run_ours(args):
         stream.synchronize()
 
         # ---- device-resident timed region ----
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-               torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         l0 = g.launch_count()
         dist_barrier(world)
         torch.cuda.synchronize(dev)
         with ClockSampler(local) as clk:
-            for k in range(args.steps):
-                flush.zero_()
-                e0, e1, e2 = ev[k]
-                e0.record(stream)
-                g.predict_all_device(1e-3 * (k + 1))
-                e1.record(stream)
-                g.force_device(N, eps2)
-                e2.record(stream)
+            step_ms, pred_ms, force_ms = timed_steps(g, stream, flush, args.steps, eps2)
             torch.cuda.synchronize(dev)
         dist_barrier(world)
         launches = g.launch_count() - l0
-        step_ms = [a.elapsed_time(c) for a, b, c in ev]
-        force_ms = [b.elapsed_time(c) for a, b, c in ev]
-        pred_ms = [a.elapsed_time(b) for a, b, c in ev]
         total_ms = dist_max(sum(step_ms), world)
         value = nint * args.steps * world / (total_ms * 1e-3) * 1e-9
 
         # ---- end to end through the C ABI with host buffers ----
-        out = np.empty((N, 6))
+        out = np.empty((N, F))
         g.set_stream(None)
         for _ in range(2):
             g.set_jp_records(rec)
@@ -312,14 +332,14 @@ def run_ours(args):
         e2e_s = dist_max(time.perf_counter() - t0, world)
         e2e = nint * args.steps * world / e2e_s * 1e-9
 
-        # ---- block-step latency through the C ABI (predict_all + force) ----
+        # ---- block-step latency through the C ABI (set_jp + predict_all + force) ----
         block_us = {}
-        for nact in (1, 32, 1024, 8192, N):
-            buf = np.empty((nact, 6))
+        for nact in (1, 32, 1024, 8192, 65536):
+            buf = np.empty((nact, F))
             for _ in range(3):
                 g.predict_all(0.0)
                 g.calc_force_on_first_nact(nact, eps2, buf)
-            reps = 50 if nact < N else 5
+            reps = 50 if nact <= 8192 else 5
             t0 = time.perf_counter()
             for _ in range(reps):
                 g.set_jp_records(rec[:nact])
@@ -328,18 +348,47 @@ def run_ours(args):
             block_us[str(nact)] = (time.perf_counter() - t0) / reps * 1e6
         g.close()
 
+        # ---- the same step with the mixed-precision kernel ----
+        gm = Gravity(ORDER, N, "mixed")
+        gm.set_stream(stream.cuda_stream)
+        gm.set_jp_records(rec)
+        gm.upload()
+        for _ in range(args.warmup):
+            gm.predict_all_device(0.0)
+            gm.force_device(N, eps2)
+        stream.synchronize()
+        mstep_ms, mpred_ms, mforce_ms = timed_steps(gm, stream, flush, args.steps, eps2)
+        gm.close()
+
     fp64_peak = measure_fma_peak(0)      # GFLOP/s, same device, same run
     fp32_peak = measure_fma_peak(2)
     force_avg_ms = sum(force_ms) / len(force_ms)
     achieved = nint * FLOPS[ORDER] / (force_avg_ms * 1e-3) * 1e-12
-    traffic = traffic_from_profiles()
+    mforce_avg_ms = sum(mforce_ms) / len(mforce_ms)
+    machieved = nint * FLOPS[ORDER] / (mforce_avg_ms * 1e-3) * 1e-12
+    mvalue = nint * args.steps / (sum(mstep_ms) * 1e-3) * 1e-9
+    traffic = traffic_from_profiles("force_fp64_o6_n262144.txt")
+    mtraffic = traffic_from_profiles("force_mixed_o6_n262144.txt")
 
-    mixed = mixed_vs_fp64(dev, stream) if not args.skip_mixed else None
+    accuracy = accuracy_leg("c3") if not args.skip_mixed else None
+    mixed = {
+        "value": mvalue, "unit": UNIT, "ms_per_step": sum(mstep_ms) / args.steps,
+        "speedup_vs_fp64": mvalue / value * world, "force_ms": mforce_avg_ms,
+        "force_speedup_vs_fp64": force_avg_ms / mforce_avg_ms,
+        "kernel_ms": {"predict": sum(mpred_ms) / len(mpred_ms), "force": mforce_avg_ms},
+        "roofline": {"bound": "fp32", "achieved": machieved, "peak": fp32_peak * 1e-3,
+                     "unit": "TFLOP/s", "frac": machieved / (fp32_peak * 1e-3), "traffic": mtraffic,
+                     "kernel": "hb::force_kernel<6, MIXED>",
+                     "peak_source": "packed-FP32 (f32x2) FMA-chain kernel measured in this run"},
+        "force_error_vs_oracle": accuracy,
+    }
+    c4 = config_c4_leg() if not args.skip_mixed else None
+    noise = noise_leg(accuracy) if not args.skip_mixed else None
     integ = device_integrator_leg() if not args.skip_integrator else None
+    mixed_int = mixed_integration_leg() if not args.skip_integrator else None
     ref_gpu = reference_gpu_leg() if not args.skip_integrator else None
     ens = ensemble_leg() if not args.skip_integrator else None
     ens_small = small_ensemble_leg() if not args.skip_integrator else None
-    mixed8 = mixed_vs_fp64_o8() if not args.skip_mixed else None
     pred = predictor_leg() if not args.skip_mixed else None
 
     if rank != 0:
@@ -351,11 +400,10 @@ def run_ours(args):
             from oracle import ref_available
             if ref_available("avx", ORDER):
                 threads = host_threads()
-                rate, times = reference_force_rate(ORDER, N, N, threads, rec)
+                rate, times = reference_force_rate(ORDER, N, CPU_NACT, threads, rec)
                 cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
-                       "sample": f"reference AVX2 Gravity (SRC/hermite4-avx.h, built from source): "
-                                 f"set_jp + predict_all + force on all {N} particles (the full "
-                                 f"step), {len(times)} steps, {sum(times):.1f} s total"}
+                       "sample": "reference AVX2 Gravity (SRC/hermite6-avx.h, built from source): "
+                                 + cpu_sample_text(len(times), f", {sum(times):.1f} s total")}
         except Exception as e:          # the baseline is reported, not required
             cpu = {"value": None, "unit": UNIT, "cores": host_threads(), "kind": "reference",
                    "sample": f"failed: {e}"}
@@ -371,27 +419,29 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(),
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": N * 14 * 8,
-                "d2h_bytes_per_step": N * 6 * 8},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": N * (8 + 3 * (ORDER - 2)) * 8,
+                "d2h_bytes_per_step": N * F * 8},
         "gpu_launches": launches,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak * 1e-3,
                      "unit": "TFLOP/s", "frac": achieved / (fp64_peak * 1e-3), "traffic": traffic,
-                     "kernel": "hb::force_kernel<4, FP64>",
+                     "kernel": "hb::force_kernel<6, FP64>",
                      "peak_source": "FP64 FMA-chain kernel measured in this run "
                                     "(hb_measure_fma_peak); MEASURED_PEAKS.json has no FP64 figure",
                      "achieved_basis": f"N^2 x {FLOPS[ORDER]} flops per launch / mean CUDA-event "
                                        "duration of the force launch"},
         "kernel_ms": {"predict": sum(pred_ms) / len(pred_ms), "force": force_avg_ms},
         "fp32_peak_tflops": fp32_peak * 1e-3,
+        "mixed": mixed,
         "block_step_us": {"order": ORDER, "nbody": N, "precision": "fp64",
                           "through": "set_jp(nact) + predict_all + calc_force_on_first_nact",
                           "us": block_us},
-        "mixed_vs_fp64": mixed,
+        "config_c4": c4,
+        "mixed_force_noise": noise,
         "device_integrator": integ,
+        "mixed_integration": mixed_int,
         "reference_gpu_recompiled": ref_gpu,
         "ensemble": ens,
         "ensemble_small_clusters": ens_small,
-        "mixed_vs_fp64_o8": mixed8,
         "predictor_roofline": pred,
         "ensemble_cpu_reference": ens_cpu,
         "clocks": clk.summary(),
@@ -401,17 +451,76 @@ def run_ours(args):
     dist_barrier(world)
 
 
-def mixed_vs_fp64(dev, stream):
-    """6th order, Plummer N = 262144, eps = 1/4096: full N^2 force in the
-    mixed-precision and FP64 kernels, and the per-particle relative force
-    error of the mixed kernel against the FP64 kernel on a 4096-particle
-    sample."""
+# ---------------------------------------------------------------------------
+STATE_CONFIGS = {
+    # name -> (order, N, eps, eta, eta_s, dtmax, t_run)
+    "c1": (4, 1024, 1 / 256, 0.01, 0.0025, 1 / 8, 1 / 8),
+    "c3": (6, 262144, 1 / 4096, 0.1, 0.02, 1 / 32, 1 / 1024),
+    "c4": (8, 1 << 20, 1 / 16384, 0.2, 0.04, 1 / 64, 1 / 4096),
+}
+
+
+def integrator_state(name):
+    """Records (slot order), time and eps2 of the FP64 device integrator after
+    its start-up and a short run: realistic acc/jrk/snp/crk and tlast."""
+    from hermite_b200 import Gravity
+    from hermite_b200.ic import plummer, records
+    order, n, eps, eta, eta_s, dtmax, t_run = STATE_CONFIGS[name]
+    with Gravity(order, n, "fp64") as g:
+        g.set_jp_records(records(plummer(n, 0), order))
+        g.integrator_init(0.0, eps * eps, eta, eta_s, dtmax)
+        g.integrator_run(t_run)
+        t = g.integrator_stats()[2]
+        rec = g.get_records()
+    return rec, t, eps * eps
+
+
+def error_stats(got, ref):
+    a = got.reshape(got.shape[0], -1, 3)
+    b = ref.reshape(ref.shape[0], -1, 3)
+    err = np.linalg.norm(a - b, axis=2) / np.linalg.norm(b, axis=2)
+    names = ("acc", "jrk", "snp", "crk")[:err.shape[1]]
+    return {nm: {"max": float(err[:, k].max()), "p99": float(np.quantile(err[:, k], 0.99)),
+                 "median": float(np.median(err[:, k]))} for k, nm in enumerate(names)}
+
+
+def accuracy_leg(name, nsample=NSAMPLE):
+    """Per-derivative relative force errors of both precisions against the
+    FP64 oracle (oracle/hermite_oracle.c, all host cores), on the first
+    nsample slots of a random permutation of an integrator state, each
+    against all N, predicted to the integrator's time."""
+    from hermite_b200 import Gravity
+    from oracle import Oracle
+    order = STATE_CONFIGS[name][0]
+    rec, t, eps2 = integrator_state(name)
+    n = rec.shape[0]
+    rng = np.random.default_rng(1)
+    pick = rng.choice(n, size=nsample, replace=False)
+    recp = np.ascontiguousarray(rec[np.concatenate([pick, np.setdiff1d(np.arange(n), pick)])])
+    t0 = time.perf_counter()
+    ref = Oracle().predict_force(order, recp, t, nsample, eps2)
+    oracle_s = time.perf_counter() - t0
+    out = {"config": name, "order": order, "nbody": n, "t": t, "sample_i": nsample,
+           "state": "FP64 device integrator after start-up and a run to t",
+           "oracle_s": oracle_s}
+    for prec in ("fp64", "mixed"):
+        with Gravity(order, n, prec) as g:
+            g.set_jp_records(recp)
+            g.predict_all(t)
+            out[prec] = error_stats(g.calc_force_on_first_nact(nsample, eps2), ref)
+    return out
+
+
+def config_c4_leg(nrate=32768):
+    """8th order, Plummer N = 2^20, eps = 1/16384 (the 8th-order
+    configuration): both kernels' rates on the first nrate i against all N,
+    and both precisions' errors against the oracle on an integrator state."""
     import torch
     from hermite_b200 import Gravity
-    order, n, eps2, reps = 6, 262144, (1.0 / 4096) ** 2, 2
-    rec = plummer_records(order, n, seed=7)
-    res = {"order": order, "nbody": n, "eps": 1.0 / 4096, "flops_per_interaction": FLOPS[order]}
-    forces = {}
+    order, n, eps2 = 8, 1 << 20, (1.0 / 16384) ** 2
+    rec = plummer_records(order, n, seed=11)
+    res = {"order": order, "nbody": n, "eps": 1.0 / 16384, "rate_i": nrate}
+    stream = torch.cuda.Stream()
     for prec in ("fp64", "mixed"):
         with torch.cuda.stream(stream):
             g = Gravity(order, n, prec)
@@ -419,25 +528,75 @@ def mixed_vs_fp64(dev, stream):
             g.set_jp_records(rec)
             g.upload()
             g.predict_all_device(0.0)
-            g.force_device(n, eps2)
+            g.force_device(nrate, eps2)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for _ in range(reps):
-                g.force_device(n, eps2)
+            for _ in range(2):
+                g.force_device(nrate, eps2)
             e1.record(stream)
             stream.synchronize()
-            ms = e0.elapsed_time(e1) / reps
-            g.set_stream(None)
-            forces[prec] = g.calc_force_on_first_nact(4096, eps2)
+            ms = e0.elapsed_time(e1) / 2
             g.close()
-        rate = float(n) * n / (ms * 1e-3) * 1e-9
-        res[prec] = {"gint_s": rate, "tflops": rate * FLOPS[order] * 1e-3, "force_ms": ms}
+        res[prec] = {"gint_s": nrate * n / (ms * 1e-3) * 1e-9, "force_ms": ms}
     res["speedup"] = res["mixed"]["gint_s"] / res["fp64"]["gint_s"]
-    a, b = forces["mixed"].reshape(4096, 3, 3), forces["fp64"].reshape(4096, 3, 3)
-    err = np.linalg.norm(a - b, axis=2) / np.linalg.norm(b, axis=2)
-    res["rel_err_vs_fp64"] = {name: {"max": float(err[:, k].max()), "median": float(np.median(err[:, k]))}
-                              for k, name in enumerate(("acc", "jrk", "snp"))}
+    res["force_error_vs_oracle"] = accuracy_leg("c4")
     return res
+
+
+def noise_leg(c3_accuracy):
+    """The mixed kernel's force deviation from the FP64 kernel on the same
+    predicted states, next to the force noise the reference's step criterion
+    tolerates (measured on the CPU by tests/test_noise_tolerance.py: white
+    noise of that relative size per derivative leaves the block steps within
+    10 %; ten times more blows them up).  c1: all 1024 particles of the
+    4th-order configuration after t = 1/8; c3: the accuracy sample."""
+    from hermite_b200 import Gravity
+    rec, t, eps2 = integrator_state("c1")
+    n = rec.shape[0]
+    f = {}
+    for prec in ("fp64", "mixed"):
+        with Gravity(4, n, prec) as g:
+            g.set_jp_records(rec)
+            g.predict_all(t)
+            f[prec] = g.calc_force_on_first_nact(n, eps2)
+    return {
+        "c1_mixed_vs_fp64": error_stats(f["mixed"], f["fp64"]),
+        "c3_mixed_vs_oracle": c3_accuracy["mixed"] if c3_accuracy else None,
+        "tolerated_relative_noise": {
+            "4th order, eta=0.01 (c1)": 1e-9, "4th order, eta=0.1 (RUN/inp.4th)": 1e-6,
+            "6th order, eta=0.1 (c3 parameters, N=4096)": 1e-11},
+        "source": "tests/test_noise_tolerance.py (reference integrator on the CPU, seeded "
+                  "relative noise on the oracle's forces)"}
+
+
+def mixed_integration_leg():
+    """4th order at the reference's own run parameters (RUN/inp.4th: eta =
+    0.1, eta_s = 0.01, dtmax = 1/16), Plummer N = 1024 and 65536 (eps = 4/N),
+    t = 0..1/4 on the graph engine, FP64 and mixed forces: block steps,
+    particle steps, time per block step and the energy error."""
+    from hermite_b200 import Gravity
+    from hermite_b200.ic import plummer, records
+    out = {}
+    for n in (1024, 65536):
+        eps2 = (4.0 / n) ** 2
+        rec = records(plummer(n, 0), 4)
+        for prec in ("fp64", "mixed"):
+            with Gravity(4, n, prec) as g:
+                g.set_engine("graph")
+                g.set_jp_records(rec)
+                g.integrator_init(0.0, eps2, 0.1, 0.01, 1.0 / 16)
+                ke0, pe0 = g.energy(eps2)
+                t0 = time.perf_counter()
+                g.integrator_run(0.25)
+                wall = time.perf_counter() - t0
+                ps, bs, _ = g.integrator_stats()
+                ke, pe = g.energy(eps2)
+            e0 = ke0 + pe0
+            out[f"n{n}_{prec}"] = {"block_steps": bs, "particle_steps": ps,
+                                   "us_per_block": wall / max(bs, 1) * 1e6,
+                                   "gint_s": ps * n / wall * 1e-9,
+                                   "de_global": (e0 - (ke + pe)) / e0}
+    return out
 
 
 def hbm_peak():
@@ -490,44 +649,6 @@ def predictor_leg(reps=50):
     return out
 
 
-def mixed_vs_fp64_o8(nsample=4096, nrate=32768):
-    """8th order, Plummer N = 1048576, eps = 1/16384 (the 8th-order
-    configuration): per-particle relative errors of the mixed-precision force
-    against the FP64 force on the first nsample particles (against all N),
-    and both kernels' rates on the first nrate particles."""
-    import torch
-    from hermite_b200 import Gravity
-    order, n, eps2 = 8, 1 << 20, (1.0 / 16384) ** 2
-    rec = plummer_records(order, n, seed=11)
-    res = {"order": order, "nbody": n, "eps": 1.0 / 16384, "sample_i": nsample, "rate_i": nrate}
-    forces = {}
-    stream = torch.cuda.Stream()
-    for prec in ("fp64", "mixed"):
-        with torch.cuda.stream(stream):
-            g = Gravity(order, n, prec)
-            g.set_stream(stream.cuda_stream)
-            g.set_jp_records(rec)
-            g.upload()
-            g.predict_all_device(0.0)
-            g.force_device(nrate, eps2)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            g.force_device(nrate, eps2)
-            e1.record(stream)
-            stream.synchronize()
-            ms = e0.elapsed_time(e1)
-            g.set_stream(None)
-            forces[prec] = g.calc_force_on_first_nact(nsample, eps2)
-            g.close()
-        res[prec] = {"gint_s": nrate * n / (ms * 1e-3) * 1e-9, "force_ms": ms}
-    res["speedup"] = res["mixed"]["gint_s"] / res["fp64"]["gint_s"]
-    a, b = forces["mixed"].reshape(nsample, 4, 3), forces["fp64"].reshape(nsample, 4, 3)
-    err = np.linalg.norm(a - b, axis=2) / np.linalg.norm(b, axis=2)
-    res["rel_err_vs_fp64"] = {name: {"max": float(err[:, k].max()), "median": float(np.median(err[:, k]))}
-                              for k, name in enumerate(("acc", "jrk", "snp", "crk"))}
-    return res
-
-
 def ensemble_cpu_leg(nclusters=256, tend=1.0 / 16):
     """The reference's AVX2 integrator (oracle/_ref/avx2-6, all host cores) on
     a sample of the ensemble leg's clusters -- the smallest, median and
@@ -558,11 +679,20 @@ def ensemble_cpu_leg(nclusters=256, tend=1.0 / 16):
             "gint_s": inter / wall * 1e-9 if wall else None}
 
 
+PROFILE_CASES = {
+    # name -> (order, precision, N)
+    "fp64_o6_c3": (6, "fp64", 262144), "mixed_o6_c3": (6, "mixed", 262144),
+    "fp64_o4": (4, "fp64", 65536), "mixed_o6": (6, "mixed", 65536),
+    "fp64_o6": (6, "fp64", 65536), "mixed_o8": (8, "mixed", 65536),
+}
+
+
 def run_profile_case(case: str):
-    """One small predict + two force launches, for ncu captures:
-    fp64_o4 = the headline kernel (4th order FP64, N = 65536, all active);
-    mixed_o6 = 6th-order mixed precision, N = 65536, all active;
-    team_c1 = one team-kernel launch on c1 (N = 1024, 16 CTAs, t = 0..1/128)."""
+    """One predict + two force launches on all N, for ncu captures:
+    fp64_o6_c3 / mixed_o6_c3 = the headline force kernel and its mixed
+    counterpart (6th order, N = 262144: 42 MB of records, 0.1-0.25 s per
+    launch); the others at N = 65536; team_c1 = one team-kernel launch on c1
+    (N = 1024, 16 CTAs, t = 0..1/128)."""
     from hermite_b200 import Gravity
     if case == "team_c1":
         from hermite_b200.ic import plummer, records
@@ -573,36 +703,36 @@ def run_profile_case(case: str):
             g.integrator_run(1.0 / 128)
             print("profile case team_c1 done", g.integrator_stats())
         return
-    order, prec = {"fp64_o4": (4, "fp64"), "mixed_o6": (6, "mixed"),
-                   "fp64_o6": (6, "fp64"), "mixed_o8": (8, "mixed")}[case]
-    g = Gravity(order, N, prec)
-    g.set_jp_records(plummer_records(order, N))
+    order, prec, n = PROFILE_CASES[case]
+    g = Gravity(order, n, prec)
+    g.set_jp_records(plummer_records(order, n))
     g.predict_all(0.0)
     for _ in range(2):
-        g.force_device(N, EPS * EPS)
+        g.force_device(n, EPS * EPS)
     g.synchronize()
     g.close()
     print(f"profile case {case} done")
 
 
-def device_integrator_leg(configs=("c1", "c2")):
+def device_integrator_leg(configs=("c1", "c2", "c3")):
     """Block-step time of the device-resident integrator (corrector and
-    scheduler on the GPU) on the plain-FP64 configurations c1 and c2 of
-    run_app.py (eta = 0.01: the mixed path is not used at such
-    small eta, where FP32 force noise collapses the Aarseth steps): wall time
+    scheduler on the GPU) on the configurations c1, c2 and c3 of run_app.py,
+    plain FP64 (at c1/c2's eta = 0.01 and at 6th order the step criterion
+    tolerates far less force noise than the mixed kernel leaves): wall time
     per block step, particle steps x N / time, and the energy error.  c1
     (N = 1024) runs on both engines: "team" (one thread-block cluster, the
     whole loop in one kernel; the automatic choice at this N) and "graph"
     (four kernels per step over the whole GPU, 32 steps per CUDA-graph
-    replay; the automatic choice for c2)."""
+    replay; the automatic choice for c2 and c3).  c2 and c3 run windows
+    (t = 0..1/64)."""
     from hermite_b200 import Gravity
     from hermite_b200.ic import plummer, records
     from run_app import CONFIGS
     out = {}
     for name in configs:
         cfg = dict(CONFIGS[name])
-        if name == "c2":
-            cfg["tend"] = 1.0 / 64          # a window: the full run is ~1e7 block steps
+        if name in ("c2", "c3"):
+            cfg["tend"] = 1.0 / 64          # a window of the run
         order, n = cfg["order"], cfg["n"]
         eps2 = cfg["eps"] ** 2
         engines = ("team", "graph") if name == "c1" else ("auto",)
@@ -698,19 +828,20 @@ def ensemble_leg(nclusters=256, tend=1.0 / 16, precision="fp64"):
 
 
 def reference_gpu_leg():
-    """The reference's own FP64 CUDA force path (SRC/hermite4-titan.cu, written
-    for sm_35) recompiled unmodified for sm_100a (oracle/_ref/titan-4), on the
-    headline workload: its own "## Init N square" report of one full N^2
-    force evaluation at N = 65536, and its app-level block-step rate over a
-    short window of configuration c2."""
+    """The reference's own FP64 CUDA force path (SRC/hermite6-titan.cu, written
+    for sm_35) recompiled unmodified for sm_100a (oracle/_ref/titan-6), on the
+    headline configuration: its own "## Init N square" report of one full
+    N^2 force evaluation at N = 262144, and its app-level block-step rate over
+    the window t = 0..1/64 of configuration c3."""
     from run_app import APP, run
-    if not Path(str(APP["ref-gpu"]).format(order=4)).exists():
+    if not Path(str(APP["ref-gpu"]).format(order=6)).exists():
         return None
-    r = run("c2", "ref-gpu", tend=1.0 / 512)
-    return {"binary": "oracle/_ref/titan-4 (reference SRC/hermite4-titan.cu, sm_100a)",
+    r = run("c3", "ref-gpu", tend=1.0 / 64)
+    return {"binary": "oracle/_ref/titan-6 (reference SRC/hermite6-titan.cu, sm_100a)",
             "init_n2_gint_s": r["init_n2_gflops"] / FLOPS[ORDER] if r["init_n2_gflops"] else None,
             "app_us_per_block": r.get("us_per_block"), "app_gint_s": r.get("app_gint_s"),
-            "window": "c2 (N=65536, eps=1/1024, eta=0.01) t = 0..1/512"}
+            "block_steps": r.get("block_steps"), "de_global": r.get("de_global"),
+            "window": "c3 (N=262144, eps=1/4096, eta=0.1) t = 0..1/64"}
 
 
 def main():
@@ -720,11 +851,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
-    ap.add_argument("--skip-mixed", action="store_true", help="omit the mixed-vs-FP64 leg")
+    ap.add_argument("--skip-mixed", action="store_true",
+                    help="omit the accuracy, 8th-order, noise and predictor legs")
     ap.add_argument("--skip-integrator", action="store_true",
                     help="omit the device-integrator block-step leg")
-    ap.add_argument("--profile", choices=("fp64_o4", "mixed_o6", "fp64_o6", "mixed_o8", "team_c1"),
-                    help="run one small case for an ncu capture and exit")
+    ap.add_argument("--profile", choices=(*PROFILE_CASES, "team_c1"),
+                    help="run one case for an ncu capture and exit")
     args = ap.parse_args()
     if args.profile:
         run_profile_case(args.profile)
