@@ -178,7 +178,7 @@ template <int ORDER, int NI, bool REFINE>
 __device__ __forceinline__ void chunk_mixed(const float *cp, const NegI32 (&I)[NI], float2 eps2,
                                             double (&f)[NI][Frc<ORDER>::words])
 {
-    constexpr int FS = (ORDER == 8) ? 9 : Frc<ORDER>::words;   // FP32-summed words
+    constexpr int FS = Frc<ORDER>::words;
     float2 s[NI][FS];
 #pragma unroll
     for (int n = 0; n < NI; ++n)
@@ -198,22 +198,120 @@ __device__ __forceinline__ void chunk_mixed(const float *cp, const NegI32 (&I)[N
         }
         J.m = *reinterpret_cast<const float2 *>(cp + PMX_M * 32 + jl);
 #pragma unroll
-        for (int n = 0; n < NI; ++n) {
-            float2 crk[3];
-            interact_mixed<ORDER, REFINE>(I[n], J, eps2, s[n], crk);
-            if constexpr (ORDER == 8) {
-                // crackle: FP64 accumulation of every pair term
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    f[n][9 + k] += (double)crk[k].x + (double)crk[k].y;
-            }
-        }
+        for (int n = 0; n < NI; ++n) interact_mixed<ORDER, REFINE>(I[n], J, eps2, s[n]);
     }
-    // flush the FP32 partial sums into the FP64 accumulators
+    // flush the FP32 partial sums (16 pairs per lane half) into the FP64
+    // accumulators
 #pragma unroll
     for (int n = 0; n < NI; ++n)
 #pragma unroll
         for (int c = 0; c < FS; ++c) f[n][c] += (double)s[n][c].x + (double)s[n][c].y;
+}
+
+// The end of a force launch, shared by the kernels below: the WJ warps of an
+// i-group add their FP64 sums (fixed order, through shared memory); with one
+// j-slice the sums are the forces; otherwise each slice publishes its
+// partial and the last CTA of the i-tile to arrive (threadfence + arrival
+// counter) adds the S partials in slice order and resets the counter.
+template <int ORDER, int NW, int NI, int WJ, int WI, int TI>
+__device__ __forceinline__ void force_epilogue(double (&f)[NI][Frc<ORDER>::words],
+                                               unsigned char *smem, const ForceArgs &a,
+                                               int ig, int jg, int ichunk0)
+{
+    constexpr int F = Frc<ORDER>::words;
+    __shared__ unsigned s_last;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int S = gridDim.y, sl = blockIdx.y;
+    // Combine the WJ warps of each i-group (fixed order), through the ring.
+    if constexpr (WJ > 1) {
+        double *red = reinterpret_cast<double *>(smem);
+        if (jg > 0) {
+#pragma unroll
+            for (int n = 0; n < NI; ++n)
+#pragma unroll
+                for (int c = 0; c < F; ++c)
+                    red[((((jg - 1) * WI + ig) * NI + n) * F + c) * 32 + lane] = f[n][c];
+        }
+        __syncthreads();
+        if (jg == 0) {
+            for (int g = 1; g < WJ; ++g)
+#pragma unroll
+                for (int n = 0; n < NI; ++n)
+#pragma unroll
+                    for (int c = 0; c < F; ++c)
+                        f[n][c] += red[((((g - 1) * WI + ig) * NI + n) * F + c) * 32 + lane];
+        }
+    }
+
+    if (S == 1) {
+        if (jg == 0) {
+#pragma unroll
+            for (int n = 0; n < NI; ++n) {
+                const int i = (ichunk0 + n) * 32 + lane;
+                if (i < a.nact) {
+#pragma unroll
+                    for (int c = 0; c < F; ++c) a.force[(size_t)i * F + c] = f[n][c];
+                }
+            }
+        }
+        return;
+    }
+
+    // j-split across CTAs: publish this slice's partial, last CTA reduces.
+    const size_t ispan = (size_t)gridDim.x * TI;
+    if (jg == 0) {
+#pragma unroll
+        for (int n = 0; n < NI; ++n) {
+            const int i = (ichunk0 + n) * 32 + lane;
+#pragma unroll
+            for (int c = 0; c < F; ++c) a.partial[((size_t)sl * ispan + i) * F + c] = f[n][c];
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = (atomicAdd(&a.counter[blockIdx.x], 1u) == (unsigned)(S - 1));
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // Sum the S slice partials of this i-tile.  With few values per tile the
+    // slices are split among thread groups (g, g+G, g+2G, ...) and the group
+    // sums are added in group order; the order is fixed either way.
+    constexpr int T = NW * 32;
+    const int i0 = blockIdx.x * TI;
+    const int V = min(TI, a.nact - i0) * F;
+    const size_t sstride = ispan * F;
+    const double *pbase = a.partial + (size_t)i0 * F;
+    if (V >= T / 2) {
+        for (int e = tid; e < V; e += T) {
+            double sum = 0.0;
+            int s = 0;
+            for (; s + 4 <= S; s += 4) {
+                const double p0 = __ldcg(pbase + (size_t)(s + 0) * sstride + e);
+                const double p1 = __ldcg(pbase + (size_t)(s + 1) * sstride + e);
+                const double p2 = __ldcg(pbase + (size_t)(s + 2) * sstride + e);
+                const double p3 = __ldcg(pbase + (size_t)(s + 3) * sstride + e);
+                sum += p0; sum += p1; sum += p2; sum += p3;
+            }
+            for (; s < S; ++s) sum += __ldcg(pbase + (size_t)s * sstride + e);
+            a.force[(size_t)i0 * F + e] = sum;
+        }
+    } else {
+        const int G = T / V;
+        const int g = tid / V, e = tid % V;
+        double *red = reinterpret_cast<double *>(smem);   // the ring is idle now
+        if (g < G) {
+            double sum = 0.0;
+            for (int s = g; s < S; s += G) sum += __ldcg(pbase + (size_t)s * sstride + e);
+            red[tid] = sum;
+        }
+        __syncthreads();
+        if (tid < V) {
+            double sum = red[tid];
+            for (int gg = 1; gg < G; ++gg) sum += red[gg * V + tid];
+            a.force[(size_t)i0 * F + tid] = sum;
+        }
+    }
+    if (tid == 0) a.counter[blockIdx.x] = 0u;
 }
 
 // Mixed precision: one Newton step on the hardware rsqrt measured no more
@@ -234,7 +332,6 @@ force_kernel(ForceArgs a)
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::body_bytes);
     unsigned char *ptile = smem + Sh::ring_bytes;          // fused only
     constexpr int RB = Rec<ORDER>::bytes;
-    __shared__ unsigned s_last;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ig = warp % WI, jg = warp / WI;
@@ -346,96 +443,170 @@ force_kernel(ForceArgs a)
         return;
     }
 
-    // Combine the WJ warps of each i-group (fixed order), through the ring.
-    if constexpr (WJ > 1) {
-        double *red = reinterpret_cast<double *>(smem);
-        if (jg > 0) {
-#pragma unroll
-            for (int n = 0; n < NI; ++n)
-#pragma unroll
-                for (int c = 0; c < F; ++c)
-                    red[((((jg - 1) * WI + ig) * NI + n) * F + c) * 32 + lane] = f[n][c];
+    force_epilogue<ORDER, NW, NI, WJ, WI, TI>(f, smem, a, ig, jg, ichunk0);
+}
+
+
+// ---------------------------------------------------------------------------
+// Mixed precision on both arithmetic pipes ("dual-pipe" shapes).
+//
+// The mixed-precision interaction keeps the FP32 FMA pipe busy and leaves the
+// FP64 pipe -- half the FP32 rate on B200 -- idle.  Here each i-group has W32
+// warps working in mixed precision and W64 warps working in FP64 on the same
+// i-particles: of every j tile of TCH chunks, the first TCH - Q64 chunks come
+// from the mixed predicted array and go to the FP32 warps, the last Q64 from
+// the FP64 predicted array (written by the predictor next to the mixed one)
+// and go to the FP64 warps, so both pipes work at once.  The partial sums
+// meet in FP64 (force_epilogue).  A partial last tile of cnt chunks keeps the
+// proportion: cnt*Q64/TCH FP64 chunks (rounded down) at its end.  The
+// split of j between the precisions is fixed by slot, so results are
+// deterministic for a launch shape; every FP64 pair is at least as accurate
+// as the mixed one it replaces.
+template <int ORDER, int NW, int NI, int W32, int W64, int TCH, int Q64>
+struct HybShape {
+    static constexpr int F = Frc<ORDER>::words;
+    static constexpr int WJ = W32 + W64;
+    static constexpr int WI = NW / WJ;
+    static constexpr int TI = WI * 32 * NI;
+    static constexpr int STG = 2;
+    static constexpr int CB32 = PredMx<ORDER>::chunk_bytes;
+    static constexpr int CB64 = Pred64<ORDER>::chunk_bytes;
+    static constexpr int off64 = (TCH - Q64) * CB32;      // FP64 chunks of a tile
+    static constexpr int tile_bytes = off64 + Q64 * CB64;
+    static constexpr int ring_bytes = STG * tile_bytes;
+    static constexpr int red_bytes = (WJ - 1) * WI * NI * F * 32 * 8;
+    static constexpr int body_bytes = ring_bytes > red_bytes ? ring_bytes : red_bytes;
+    static constexpr int smem_bytes = body_bytes + 64;
+    static_assert(NW % WJ == 0 && W32 >= 1 && W64 >= 1, "warp roles");
+    static_assert(Q64 >= 1 && Q64 < TCH, "both precisions in every full tile");
+    static_assert(256 % TI == 0, "i-tile must divide the slot padding");
+    static_assert(CB32 % 16 == 0 && CB64 % 16 == 0 && off64 % 16 == 0, "bulk-copy alignment");
+};
+
+// FP64 chunks among the cnt chunks of a tile.
+template <int TCH, int Q64>
+__device__ __forceinline__ int hyb_n64(int cnt) { return (cnt * Q64) / TCH; }
+
+// The tile loop of one warp role.  Every warp of the CTA runs the same
+// barrier sequence (one bounded wait + __syncthreads_and, then
+// __syncthreads, per tile); only the chunks they compute differ.  Returns
+// the tile whose wait gave up, or -1.
+template <int ORDER, int NW, int NI, int W32, int W64, int TCH, int Q64, bool FP64ROLE,
+          bool REFINE, class IBody>
+__device__ __forceinline__ int hyb_tiles(const ForceArgs &a, unsigned char *smem, uint64_t *bar,
+                                         int c0, int c1, int ntile, int jq, const IBody (&I)[NI],
+                                         double (&f)[NI][Frc<ORDER>::words])
+{
+    using Sh = HybShape<ORDER, NW, NI, W32, W64, TCH, Q64>;
+    const float2 eps2f = f2((float)a.eps2);
+    for (int t = 0; t < ntile; ++t) {
+        const int st = t % Sh::STG;
+        const bool got = mbar_wait_bounded(&bar[st], (uint32_t)((t / Sh::STG) & 1), a.spin);
+        if (!__syncthreads_and(got)) return t;
+        const int cnt = min(TCH, c1 - (c0 + t * TCH));
+        const int n64 = hyb_n64<TCH, Q64>(cnt);
+        const unsigned char *tile = smem + st * Sh::tile_bytes;
+        if constexpr (FP64ROLE) {
+            for (int q = jq; q < n64; q += W64)
+                chunk64<ORDER, NI>(reinterpret_cast<const double *>(tile + Sh::off64 + q * Sh::CB64),
+                                   I, a.eps2, f);
+        } else {
+            for (int q = jq; q < cnt - n64; q += W32)
+                chunk_mixed<ORDER, NI, REFINE>(reinterpret_cast<const float *>(tile + q * Sh::CB32),
+                                               I, eps2f, f);
         }
         __syncthreads();
-        if (jg == 0) {
-            for (int g = 1; g < WJ; ++g)
+        if (threadIdx.x == 0 && t + Sh::STG < ntile) {
+            // issue tile t + STG into the stage just released
+            const int cs = c0 + (t + Sh::STG) * TCH;
+            const int cn = min(TCH, c1 - cs);
+            const int m64 = hyb_n64<TCH, Q64>(cn), m32 = cn - m64;
+            unsigned char *dst = smem + st * Sh::tile_bytes;
+            mbar_arrive_expect_tx(&bar[st], (uint32_t)(m32 * Sh::CB32 + m64 * Sh::CB64));
+            if (m32 > 0)
+                bulk_load(dst, static_cast<const unsigned char *>(a.pred) + (size_t)cs * Sh::CB32,
+                          (uint32_t)(m32 * Sh::CB32), &bar[st]);
+            if (m64 > 0)
+                bulk_load(dst + Sh::off64,
+                          static_cast<const unsigned char *>(a.pred64) + (size_t)(cs + m32) * Sh::CB64,
+                          (uint32_t)(m64 * Sh::CB64), &bar[st]);
+        }
+    }
+    return -1;
+}
+
+template <int ORDER, int NW, int NI, int W32, int W64, int TCH, int Q64, int MINB,
+          bool REFINE = (HB_MIXED_REFINE != 0)>
+__global__ void __launch_bounds__(NW * 32, MINB)
+force_kernel_hyb(ForceArgs a)
+{
+    using Sh = HybShape<ORDER, NW, NI, W32, W64, TCH, Q64>;
+    constexpr int F = Sh::F, WI = Sh::WI, TI = Sh::TI, STG = Sh::STG, WJ = Sh::WJ;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::body_bytes);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ig = warp % WI, jg = warp / WI;
+    const int S = gridDim.y, sl = blockIdx.y;
+    const int c0 = (int)(((long long)sl * a.nchunk) / S);
+    const int c1 = (int)(((long long)(sl + 1) * a.nchunk) / S);
+    const int ntile = (c1 - c0 + TCH - 1) / TCH;
+    const int ichunk0 = (blockIdx.x * TI) / 32 + ig * NI;
+
+    double f[NI][F];
 #pragma unroll
-                for (int n = 0; n < NI; ++n)
+    for (int n = 0; n < NI; ++n)
 #pragma unroll
-                    for (int c = 0; c < F; ++c)
-                        f[n][c] += red[((((g - 1) * WI + ig) * NI + n) * F + c) * 32 + lane];
+        for (int c = 0; c < F; ++c) f[n][c] = 0.0;
+
+    if (tid == 0) {
+#pragma unroll
+        for (int st = 0; st < STG; ++st) mbar_init(&bar[st], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int t = 0; t < STG && t < ntile; ++t) {
+            const int cs = c0 + t * TCH, cn = min(TCH, c1 - cs);
+            const int m64 = hyb_n64<TCH, Q64>(cn), m32 = cn - m64;
+            unsigned char *dst = smem + t * Sh::tile_bytes;
+            mbar_arrive_expect_tx(&bar[t], (uint32_t)(m32 * Sh::CB32 + m64 * Sh::CB64));
+            if (m32 > 0)
+                bulk_load(dst, static_cast<const unsigned char *>(a.pred) + (size_t)cs * Sh::CB32,
+                          (uint32_t)(m32 * Sh::CB32), &bar[t]);
+            if (m64 > 0)
+                bulk_load(dst + Sh::off64,
+                          static_cast<const unsigned char *>(a.pred64) + (size_t)(cs + m32) * Sh::CB64,
+                          (uint32_t)(m64 * Sh::CB64), &bar[t]);
         }
     }
 
-    if (S == 1) {
-        if (jg == 0) {
+    int failed_at;
+    if (jg >= W32) {
+        Body64 I[NI];
 #pragma unroll
-            for (int n = 0; n < NI; ++n) {
-                const int i = (ichunk0 + n) * 32 + lane;
-                if (i < a.nact) {
+        for (int n = 0; n < NI; ++n)
+            load_i64<ORDER>(static_cast<const double *>(a.pred64), ichunk0 + n, lane, I[n]);
+        failed_at = hyb_tiles<ORDER, NW, NI, W32, W64, TCH, Q64, true, REFINE>(
+            a, smem, bar, c0, c1, ntile, jg - W32, I, f);
+    } else {
+        NegI32 I[NI];
 #pragma unroll
-                    for (int c = 0; c < F; ++c) a.force[(size_t)i * F + c] = f[n][c];
-                }
-            }
+        for (int n = 0; n < NI; ++n)
+            load_i_mixed<ORDER>(static_cast<const float *>(a.pred), ichunk0 + n, lane, I[n]);
+        failed_at = hyb_tiles<ORDER, NW, NI, W32, W64, TCH, Q64, false, REFINE>(
+            a, smem, bar, c0, c1, ntile, jg, I, f);
+    }
+    if (failed_at >= 0) {
+        // Leave no bulk copy writing into this CTA's shared memory after exit.
+        if (tid == 0) {
+            raise_error(a.err, kErrWaitTimeout);
+            for (int t = failed_at; t < ntile && t < failed_at + STG; ++t)
+                mbar_wait_bounded(&bar[t % STG], (uint32_t)((t / STG) & 1));
         }
         return;
     }
-
-    // j-split across CTAs: publish this slice's partial, last CTA reduces.
-    const size_t ispan = (size_t)gridDim.x * TI;
-    if (jg == 0) {
-#pragma unroll
-        for (int n = 0; n < NI; ++n) {
-            const int i = (ichunk0 + n) * 32 + lane;
-#pragma unroll
-            for (int c = 0; c < F; ++c) a.partial[((size_t)sl * ispan + i) * F + c] = f[n][c];
-        }
-    }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) s_last = (atomicAdd(&a.counter[blockIdx.x], 1u) == (unsigned)(S - 1));
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    // Sum the S slice partials of this i-tile.  With few values per tile the
-    // slices are split among thread groups (g, g+G, g+2G, ...) and the group
-    // sums are added in group order; the order is fixed either way.
-    constexpr int T = NW * 32;
-    const int i0 = blockIdx.x * TI;
-    const int V = min(TI, a.nact - i0) * F;
-    const size_t sstride = ispan * F;
-    const double *pbase = a.partial + (size_t)i0 * F;
-    if (V >= T / 2) {
-        for (int e = tid; e < V; e += T) {
-            double sum = 0.0;
-            int s = 0;
-            for (; s + 4 <= S; s += 4) {
-                const double p0 = __ldcg(pbase + (size_t)(s + 0) * sstride + e);
-                const double p1 = __ldcg(pbase + (size_t)(s + 1) * sstride + e);
-                const double p2 = __ldcg(pbase + (size_t)(s + 2) * sstride + e);
-                const double p3 = __ldcg(pbase + (size_t)(s + 3) * sstride + e);
-                sum += p0; sum += p1; sum += p2; sum += p3;
-            }
-            for (; s < S; ++s) sum += __ldcg(pbase + (size_t)s * sstride + e);
-            a.force[(size_t)i0 * F + e] = sum;
-        }
-    } else {
-        const int G = T / V;
-        const int g = tid / V, e = tid % V;
-        double *red = reinterpret_cast<double *>(smem);   // the ring is idle now
-        if (g < G) {
-            double sum = 0.0;
-            for (int s = g; s < S; s += G) sum += __ldcg(pbase + (size_t)s * sstride + e);
-            red[tid] = sum;
-        }
-        __syncthreads();
-        if (tid < V) {
-            double sum = red[tid];
-            for (int gg = 1; gg < G; ++gg) sum += red[gg * V + tid];
-            a.force[(size_t)i0 * F + tid] = sum;
-        }
-    }
-    if (tid == 0) a.counter[blockIdx.x] = 0u;
+    force_epilogue<ORDER, NW, NI, WJ, WI, TI>(f, smem, a, ig, jg, ichunk0);
 }
 
 }  // namespace hb

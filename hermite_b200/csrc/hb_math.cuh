@@ -186,12 +186,11 @@ __device__ __forceinline__ float2 rsqrt2(float2 x)
     return y;
 }
 
-// Accumulates into s[] (FP32, packed over the two j) for acc, jrk [, snp];
-// at 8th order the crackle of the pair is returned in crk[] (FP32, packed)
-// for the caller to add into FP64.
+// Accumulates into s[] (FP32, packed over the two j) for acc, jrk [, snp
+// [, crk]]; the caller flushes these partial sums into FP64 accumulators.
 template <int ORDER, bool REFINE>
 __device__ __forceinline__ void interact_mixed(const NegI32 &I, const JPair32 &J,
-                                               float2 eps2, float2 *s, float2 *crk)
+                                               float2 eps2, float2 *s)
 {
     float2 dr[3], dv[3];
 #pragma unroll
@@ -243,7 +242,7 @@ __device__ __forceinline__ void interact_mixed(const NegI32 &I, const JPair32 &J
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const float2 w = fma2(ga3, dr[k], fma2(be9, t[k], fma2(al9, u[k], dj[k])));
-                crk[k] = mul2(mr3, w);
+                s[9 + k] = fma2(mr3, w, s[9 + k]);
             }
         }
     }

@@ -9,8 +9,11 @@ reports are parsed:
   " de(local/global) : ..."                         (SRC/nbodysystem.h:948-951)
   "ke = .., pe = .., e = .."                        (SRC/nbodysystem.h:644-647)
 
-    python run_app.py --config c1 [--impl gpu|gpu-mixed|gpu-fast|cpu-ref|ref-gpu]
-           [--tend T] [--n N]
+    python run_app.py --config c1 [--impl gpu|gpu-mixed|gpu-fast|cpu-ref|ref-gpu|
+                                         device|device-mixed] [--tend T] [--n N]
+
+--impl device[-mixed] runs the configuration on the library's device-resident
+integrator instead of the reference's host loop.
 
 Configurations (Plummer spheres from hermite_b200.ic, seed 0, equal masses,
 G = M = 1, gen-plum's scaling E ~ -1/4):
@@ -126,14 +129,56 @@ def run(config: str, impl: str = "gpu", tend: float | None = None, n: int | None
     return out
 
 
+def run_device(config: str, precision: str = "fp64", tend: float | None = None,
+               n: int | None = None, seed: int = 0, engine: str = "auto") -> dict:
+    """The same configuration on the library's device-resident integrator
+    (corrector and block-step scheduler on the GPU, hb_integrator_*): block
+    and particle steps, wall time per block step, interactions per second
+    (particle steps x N / wall) and the relative energy error at the end, with
+    the reference's sign convention (E0 - E) / E0 (SRC/nbodysystem.h:948-951)."""
+    from hermite_b200 import Gravity
+    from hermite_b200.ic import plummer, records
+    cfg = dict(CONFIGS[config])
+    if tend is not None:
+        cfg["tend"] = tend
+    if n is not None:
+        cfg["n"] = n
+    order, nb = cfg["order"], cfg["n"]
+    eps2 = cfg["eps"] ** 2
+    with Gravity(order, nb, precision) as g:
+        g.set_engine(engine)
+        used = g.engine()
+        g.set_jp_records(records(plummer(nb, seed), order))
+        t0 = time.perf_counter()
+        g.integrator_init(0.0, eps2, cfg["eta"], cfg["eta_s"], 1.0 / cfg["dtmaxinv"])
+        init_s = time.perf_counter() - t0
+        ke0, pe0 = g.energy(eps2)
+        t0 = time.perf_counter()
+        g.integrator_run(cfg["tend"])
+        wall = time.perf_counter() - t0
+        ps, bs, t = g.integrator_stats()
+        ke, pe = g.energy(eps2)
+    e0 = ke0 + pe0
+    return {"config": config, "impl": f"device-{precision}", "engine": used[0],
+            "order": order, "n": nb, "eps": cfg["eps"], "eta": cfg["eta"], "eta_s": cfg["eta_s"],
+            "dtmax": 1.0 / cfg["dtmaxinv"], "tend": cfg["tend"], "t": t, "init_s": init_s,
+            "wall_s": wall, "block_steps": bs, "particle_steps": ps,
+            "nact_mean": ps / max(bs, 1), "us_per_block": wall / max(bs, 1) * 1e6,
+            "app_gint_s": ps * nb / wall * 1e-9, "e0": e0, "de_global": (e0 - (ke + pe)) / e0}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
-    ap.add_argument("--impl", default="gpu", choices=sorted(APP))
+    ap.add_argument("--impl", default="gpu", choices=sorted(APP) + ["device", "device-mixed"])
     ap.add_argument("--tend", type=float, default=None)
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--threads", type=int, default=None)
     a = ap.parse_args()
+    if a.impl.startswith("device"):
+        prec = "mixed" if a.impl == "device-mixed" else "fp64"
+        print(json.dumps(run_device(a.config, prec, a.tend, a.n)))
+        return
     print(json.dumps(run(a.config, a.impl, a.tend, a.n, threads=a.threads)))
 
 
