@@ -724,7 +724,7 @@ def device_integrator_leg(configs=("c1", "c2", "c3")):
     whole loop in one kernel; the automatic choice at this N) and "graph"
     (four kernels per step over the whole GPU, 32 steps per CUDA-graph
     replay; the automatic choice for c2 and c3).  c2 and c3 run windows
-    (t = 0..1/64)."""
+    (t = 0..1/64 and 0..1/32)."""
     from hermite_b200 import Gravity
     from hermite_b200.ic import plummer, records
     from run_app import CONFIGS
@@ -732,7 +732,8 @@ def device_integrator_leg(configs=("c1", "c2", "c3")):
     for name in configs:
         cfg = dict(CONFIGS[name])
         if name in ("c2", "c3"):
-            cfg["tend"] = 1.0 / 64          # a window of the run
+            # windows of the runs (c3: the reference CUDA leg's window)
+            cfg["tend"] = 1.0 / 64 if name == "c2" else 1.0 / 32
         order, n = cfg["order"], cfg["n"]
         eps2 = cfg["eps"] ** 2
         engines = ("team", "graph") if name == "c1" else ("auto",)
@@ -832,16 +833,16 @@ def reference_gpu_leg():
     for sm_35) recompiled unmodified for sm_100a (oracle/_ref/titan-6), on the
     headline configuration: its own "## Init N square" report of one full
     N^2 force evaluation at N = 262144, and its app-level block-step rate over
-    the window t = 0..1/64 of configuration c3."""
+    the window t = 0..1/32 of configuration c3."""
     from run_app import APP, run
     if not Path(str(APP["ref-gpu"]).format(order=6)).exists():
         return None
-    r = run("c3", "ref-gpu", tend=1.0 / 64)
+    r = run("c3", "ref-gpu", tend=1.0 / 32)
     return {"binary": "oracle/_ref/titan-6 (reference SRC/hermite6-titan.cu, sm_100a)",
             "init_n2_gint_s": r["init_n2_gflops"] / FLOPS[ORDER] if r["init_n2_gflops"] else None,
             "app_us_per_block": r.get("us_per_block"), "app_gint_s": r.get("app_gint_s"),
             "block_steps": r.get("block_steps"), "de_global": r.get("de_global"),
-            "window": "c3 (N=262144, eps=1/4096, eta=0.1) t = 0..1/64"}
+            "window": "c3 (N=262144, eps=1/4096, eta=0.1) t = 0..1/32"}
 
 
 def main():

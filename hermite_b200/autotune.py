@@ -10,7 +10,8 @@ library compiles in (hb_capi.cu looks up the nearest bucket).
                                     [--json results.json] [--quick]
                                     [--orders 4,6,8] [--precisions fp64,mixed]
                                     [--n-buckets 65536] [--nact-buckets 2,8,32]
-                                    [--merge]
+                                    [--merge] [--max-interactions X]
+                                    [--variants 0,1,20] [--trials-json all.json]
 
 --merge keeps the existing table and replaces or adds only the measured
 (order, precision, N bucket, nact bucket) entries.
@@ -73,7 +74,10 @@ def s_candidates(nact, n, nsm, ti):
     return sorted(cands)
 
 
-def tune(orders, precisions, n_buckets, nact_buckets, quick=False, log=print):
+def tune(orders, precisions, n_buckets, nact_buckets, quick=False, log=print,
+         max_interactions=MAX_INTERACTIONS, variants=None, trials=None):
+    """variants: restrict the timed shapes to these indices (None: all);
+    trials: a list that receives every (shape, slice count) timing."""
     import torch
     from hermite_b200 import Gravity, load_library
     import ctypes
@@ -100,16 +104,22 @@ def tune(orders, precisions, n_buckets, nact_buckets, quick=False, log=print):
                     g.upload()
                     g.predict_all_device(0.0)
                     for nact in nact_buckets:
-                        if nact > n or nact * n > MAX_INTERACTIONS:
+                        if nact > n or nact * n > max_interactions:
                             continue
                         reps = 3 if nact * n > (1 << 30) else 7
                         best = None
                         for v in range(nvar):
+                            if variants is not None and v not in variants:
+                                continue
                             for s in s_candidates(nact, n, nsm, tis[v]):
                                 if quick and s not in (1, s_candidates(nact, n, nsm, tis[v])[-1]):
                                     continue
                                 g.set_force_shape(v, s)
                                 ms = time_force(g, stream, nact, eps2, reps)
+                                if trials is not None:
+                                    trials.append({"order": order, "precision": prec, "n": n,
+                                                   "nact": nact, "variant": v, "jsplit": s,
+                                                   "ms": ms})
                                 if best is None or ms < best[0]:
                                     best = (ms, v, s)
                         g.set_force_shape(-1, 0)
@@ -171,11 +181,20 @@ def main():
     ap.add_argument("--n-buckets", default=",".join(map(str, N_BUCKETS)))
     ap.add_argument("--nact-buckets", default=",".join(map(str, NACT_BUCKETS)))
     ap.add_argument("--merge", action="store_true", help="update only the measured entries")
+    ap.add_argument("--max-interactions", type=float, default=float(MAX_INTERACTIONS),
+                    help="skip buckets with more interactions per launch")
+    ap.add_argument("--variants", default=None, help="time only these shapes (comma list)")
+    ap.add_argument("--trials-json", default=None, help="write every timing here")
     a = ap.parse_args()
     import torch
+    trials = []
     res = tune([int(x) for x in a.orders.split(",")], a.precisions.split(","),
                [int(x) for x in a.n_buckets.split(",")], [int(x) for x in a.nact_buckets.split(",")],
-               quick=a.quick)
+               quick=a.quick, max_interactions=int(a.max_interactions),
+               variants=[int(v) for v in a.variants.split(",")] if a.variants else None,
+               trials=trials)
+    if a.trials_json:
+        Path(a.trials_json).write_text(json.dumps(trials, indent=1))
     if a.merge and Path(a.out).exists():
         merge_inc(res, Path(a.out), torch.cuda.get_device_name(0))
     else:

@@ -10,9 +10,18 @@ j-particles, predicted to the integrator's time, and the C oracle
 (oracle/hermite_oracle.c, a restatement of the reference's generic Gravity,
 SRC/hermite6.h:332-360, SRC/hermite8.h:385-425) does the same on the CPU.
 
-Bounds, per derivative (max over the sample of |f - f_oracle| / |f_oracle|):
-FP64 1e-12 (summation order only); mixed precision at about three times the
-maxima measured on a B200.
+Bounds, per derivative, on the maximum and the median over the sample of
+|f - f_oracle| / |f_oracle|:
+* FP64: 1e-12 (summation order only), except crackle at 1e-9: at a few
+  particles the crackle pair terms cancel to a millionth of their magnitude,
+  so summation-order rounding alone reaches 3.7e-10 there (median 2.6e-14;
+  B200, c4).
+* Mixed precision: about three times the maxima and medians measured on a
+  B200 (c3: acc/jrk/snp max 3.1e-7 / 5.6e-6 / 6.3e-5, median 2.0e-8 /
+  1.4e-7 / 2.8e-7; c4: max 2.2e-7 / 3.9e-6 / 1.2e-5 / 4.9e-3, median
+  1.9e-8 / 1.3e-7 / 2.8e-7 / 3.7e-7).  The median bound is what catches a
+  broken accumulation of a derivative; the maxima sit at the particles whose
+  sums cancel.
 """
 import numpy as np
 import pytest
@@ -22,9 +31,11 @@ from inputs import rel_err
 from states import CONFIGS, integrator_state, sample_first
 
 NSAMPLE = 4096
-FP64_TOL = 1e-12
 # acc, jrk, snp [, crk]
-MIXED_TOL = {"c3": (1.5e-6, 3e-5, 1e-4), "c4": (1.5e-6, 3e-5, 1e-4, 1e-4)}
+FP64_TOL = (1e-12, 1e-12, 1e-12, 1e-9)
+FP64_MEDIAN = 1e-13
+MIXED_TOL = {"c3": (1e-6, 2e-5, 2e-4), "c4": (1e-6, 1.2e-5, 4e-5, 1.5e-2)}
+MIXED_MEDIAN = {"c3": (6e-8, 5e-7, 1e-6), "c4": (6e-8, 5e-7, 1e-6, 1.2e-6)}
 T_RUN = {"c3": 1.0 / 1024, "c4": 1.0 / 4096}
 
 _cache = {}
@@ -54,5 +65,7 @@ def test_sample_against_oracle(name, precision, oracle):
     print(f"{name} {precision}: max", " ".join(f"{e:.2e}" for e in err.max(axis=0)),
           "median", " ".join(f"{e:.2e}" for e in np.median(err, axis=0)))
     for k in range(err.shape[1]):
-        tol = FP64_TOL if precision == "fp64" else MIXED_TOL[name][k]
+        tol = FP64_TOL[k] if precision == "fp64" else MIXED_TOL[name][k]
+        med = FP64_MEDIAN if precision == "fp64" else MIXED_MEDIAN[name][k]
         assert err[:, k].max() <= tol, (name, precision, k, err[:, k].max())
+        assert np.median(err[:, k]) <= med, (name, precision, k, np.median(err[:, k]))
