@@ -17,15 +17,13 @@
 
 namespace hb {
 // compiled launch shapes per order and precision (hb_force_table.cuh)
-// (FP64 tables: 20 shapes; mixed tables: the same 20 plus 4 dual-pipe shapes)
-constexpr int kNumVariants64 = 20, kNumVariants = 24;
+constexpr int kNumVariants = 20;
 const ForceVariant *force_variant_64(int order, int v);
 const ForceVariant *force_variant_mixed(int order, int v);
 
 int force_variant_count(int order, bool mixed)
 {
-    if (order == 4 || order == 6 || order == 8) return mixed ? kNumVariants : kNumVariants64;
-    return order == 9 && !mixed ? kNumVariants64 : 0;
+    return (order == 4 || order == 6 || order == 8 || (order == 9 && !mixed)) ? kNumVariants : 0;
 }
 
 const ForceVariant *force_variant(int order, bool mixed, int v)
@@ -64,8 +62,6 @@ struct hb_ctx {
     double *d_jp = nullptr, *d_force = nullptr, *d_pot = nullptr, *d_posm = nullptr;
     double *d_partial = nullptr;
     void *d_pred = nullptr;
-    void *d_pred64x = nullptr;      // FP64 layout beside the mixed one (dual-pipe shapes)
-    bool pred_has64 = false;        // d_pred64x holds the prediction at tsys
     unsigned *d_counter = nullptr;
     int *h_err = nullptr, *d_err = nullptr;
     size_t partial_cap = 0;         // doubles
@@ -286,19 +282,15 @@ int run_force(hb_ctx *ctx, int nact, double eps2, double *force_out_dev)
         const size_t smax = ctx->partial_cap / need_per_slice;
         if ((size_t)S > smax) S = (int)std::max<size_t>(1, smax);
     }
-    if (!fv->fused && (ctx->pred_stale || (fv->q64 > 0 && !ctx->pred_has64))) {
-        // two-pass shape: the predictor kernel first (for a dual-pipe shape
-        // writing the FP64 layout as well)
+    if (!fv->fused && ctx->pred_stale) {
+        // two-pass shape: the predictor kernel first
         HB_CK(launch_predict(ctx->order, mixed, ctx->d_jp, ctx->nbody, ctx->npad, ctx->tsys,
-                             ctx->d_pred, ctx->d_err, ctx->stream,
-                             fv->q64 > 0 ? ctx->d_pred64x : nullptr));
+                             ctx->d_pred, ctx->d_err, ctx->stream));
         ctx->launches++;
         ctx->pred_stale = false;
-        ctx->pred_has64 = fv->q64 > 0;
     }
     ForceArgs a{};
     a.pred = ctx->d_pred;
-    a.pred64 = ctx->d_pred64x;
     a.jp = ctx->d_jp;
     a.tsys = ctx->tsys;
     a.nbody = ctx->nbody;
@@ -412,10 +404,8 @@ int hb_create(int order, int nbody, int precision, hb_ctx **out)
     ctx->njpsend = nbody;
 
     const size_t np = ctx->npad;
-    // the predicted array (FP64 or mixed layout) and, after the mixed layout,
-    // room for the FP64 layout that the dual-pipe mixed shapes also read
-    const size_t predmx_bytes = (np * predmx_ncomp(order) * sizeof(float) + 255) / 256 * 256;
-    const size_t pred_bytes = predmx_bytes + np * pred64_ncomp(order) * sizeof(double);
+    const size_t pred_bytes = std::max(np * pred64_ncomp(order) * sizeof(double),
+                                       np * predmx_ncomp(order) * sizeof(float));
     ctx->partial_cap = (size_t)2 * ctx->nsm * 8 * 256 * ctx->F;
     bool ok = true;
     ok = ok && cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) == cudaSuccess;
@@ -433,7 +423,6 @@ int hb_create(int order, int nbody, int precision, hb_ctx **out)
     ok = ok && cudaMalloc(&ctx->d_pred, pred_bytes) == cudaSuccess;
     ok = ok && cudaMalloc((void **)&ctx->d_counter, (np / 32 + 1) * sizeof(unsigned)) == cudaSuccess;
     if (ok) {
-        ctx->d_pred64x = static_cast<unsigned char *>(ctx->d_pred) + predmx_bytes;
         ok = cudaHostGetDevicePointer((void **)&ctx->d_err, ctx->h_err, 0) == cudaSuccess &&
              cudaHostGetDevicePointer((void **)&ctx->h_force_dev, ctx->h_force, 0) == cudaSuccess;
     }
@@ -517,7 +506,6 @@ int hb_predict_all_device(hb_ctx *ctx, double tsys)
     ctx->tsys = tsys;
     ctx->pred_precision = ctx->precision;
     ctx->pred_stale = true;
-    ctx->pred_has64 = false;
     return HB_OK;
 }
 
@@ -529,7 +517,6 @@ int hb_predict_pass(hb_ctx *ctx)
                          ctx->tsys, ctx->d_pred, ctx->d_err, ctx->stream));
     ctx->launches++;
     ctx->pred_stale = false;
-    ctx->pred_has64 = false;
     return HB_OK;
 }
 

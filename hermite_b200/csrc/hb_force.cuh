@@ -447,166 +447,5 @@ force_kernel(ForceArgs a)
 }
 
 
-// ---------------------------------------------------------------------------
-// Mixed precision on both arithmetic pipes ("dual-pipe" shapes).
-//
-// The mixed-precision interaction keeps the FP32 FMA pipe busy and leaves the
-// FP64 pipe -- half the FP32 rate on B200 -- idle.  Here each i-group has W32
-// warps working in mixed precision and W64 warps working in FP64 on the same
-// i-particles: of every j tile of TCH chunks, the first TCH - Q64 chunks come
-// from the mixed predicted array and go to the FP32 warps, the last Q64 from
-// the FP64 predicted array (written by the predictor next to the mixed one)
-// and go to the FP64 warps, so both pipes work at once.  The partial sums
-// meet in FP64 (force_epilogue).  A partial last tile of cnt chunks keeps the
-// proportion: cnt*Q64/TCH FP64 chunks (rounded down) at its end.  The
-// split of j between the precisions is fixed by slot, so results are
-// deterministic for a launch shape; every FP64 pair is at least as accurate
-// as the mixed one it replaces.
-template <int ORDER, int NW, int NI, int W32, int W64, int TCH, int Q64>
-struct HybShape {
-    static constexpr int F = Frc<ORDER>::words;
-    static constexpr int WJ = W32 + W64;
-    static constexpr int WI = NW / WJ;
-    static constexpr int TI = WI * 32 * NI;
-    static constexpr int STG = 2;
-    static constexpr int CB32 = PredMx<ORDER>::chunk_bytes;
-    static constexpr int CB64 = Pred64<ORDER>::chunk_bytes;
-    static constexpr int off64 = (TCH - Q64) * CB32;      // FP64 chunks of a tile
-    static constexpr int tile_bytes = off64 + Q64 * CB64;
-    static constexpr int ring_bytes = STG * tile_bytes;
-    static constexpr int red_bytes = (WJ - 1) * WI * NI * F * 32 * 8;
-    static constexpr int body_bytes = ring_bytes > red_bytes ? ring_bytes : red_bytes;
-    static constexpr int smem_bytes = body_bytes + 64;
-    static_assert(NW % WJ == 0 && W32 >= 1 && W64 >= 1, "warp roles");
-    static_assert(Q64 >= 1 && Q64 < TCH, "both precisions in every full tile");
-    static_assert(256 % TI == 0, "i-tile must divide the slot padding");
-    static_assert(CB32 % 16 == 0 && CB64 % 16 == 0 && off64 % 16 == 0, "bulk-copy alignment");
-};
-
-// FP64 chunks among the cnt chunks of a tile.
-template <int TCH, int Q64>
-__device__ __forceinline__ int hyb_n64(int cnt) { return (cnt * Q64) / TCH; }
-
-// The tile loop of one warp role.  Every warp of the CTA runs the same
-// barrier sequence (one bounded wait + __syncthreads_and, then
-// __syncthreads, per tile); only the chunks they compute differ.  Returns
-// the tile whose wait gave up, or -1.
-template <int ORDER, int NW, int NI, int W32, int W64, int TCH, int Q64, bool FP64ROLE,
-          bool REFINE, class IBody>
-__device__ __forceinline__ int hyb_tiles(const ForceArgs &a, unsigned char *smem, uint64_t *bar,
-                                         int c0, int c1, int ntile, int jq, const IBody (&I)[NI],
-                                         double (&f)[NI][Frc<ORDER>::words])
-{
-    using Sh = HybShape<ORDER, NW, NI, W32, W64, TCH, Q64>;
-    const float2 eps2f = f2((float)a.eps2);
-    for (int t = 0; t < ntile; ++t) {
-        const int st = t % Sh::STG;
-        const bool got = mbar_wait_bounded(&bar[st], (uint32_t)((t / Sh::STG) & 1), a.spin);
-        if (!__syncthreads_and(got)) return t;
-        const int cnt = min(TCH, c1 - (c0 + t * TCH));
-        const int n64 = hyb_n64<TCH, Q64>(cnt);
-        const unsigned char *tile = smem + st * Sh::tile_bytes;
-        if constexpr (FP64ROLE) {
-            for (int q = jq; q < n64; q += W64)
-                chunk64<ORDER, NI>(reinterpret_cast<const double *>(tile + Sh::off64 + q * Sh::CB64),
-                                   I, a.eps2, f);
-        } else {
-            for (int q = jq; q < cnt - n64; q += W32)
-                chunk_mixed<ORDER, NI, REFINE>(reinterpret_cast<const float *>(tile + q * Sh::CB32),
-                                               I, eps2f, f);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0 && t + Sh::STG < ntile) {
-            // issue tile t + STG into the stage just released
-            const int cs = c0 + (t + Sh::STG) * TCH;
-            const int cn = min(TCH, c1 - cs);
-            const int m64 = hyb_n64<TCH, Q64>(cn), m32 = cn - m64;
-            unsigned char *dst = smem + st * Sh::tile_bytes;
-            mbar_arrive_expect_tx(&bar[st], (uint32_t)(m32 * Sh::CB32 + m64 * Sh::CB64));
-            if (m32 > 0)
-                bulk_load(dst, static_cast<const unsigned char *>(a.pred) + (size_t)cs * Sh::CB32,
-                          (uint32_t)(m32 * Sh::CB32), &bar[st]);
-            if (m64 > 0)
-                bulk_load(dst + Sh::off64,
-                          static_cast<const unsigned char *>(a.pred64) + (size_t)(cs + m32) * Sh::CB64,
-                          (uint32_t)(m64 * Sh::CB64), &bar[st]);
-        }
-    }
-    return -1;
-}
-
-template <int ORDER, int NW, int NI, int W32, int W64, int TCH, int Q64, int MINB,
-          bool REFINE = (HB_MIXED_REFINE != 0)>
-__global__ void __launch_bounds__(NW * 32, MINB)
-force_kernel_hyb(ForceArgs a)
-{
-    using Sh = HybShape<ORDER, NW, NI, W32, W64, TCH, Q64>;
-    constexpr int F = Sh::F, WI = Sh::WI, TI = Sh::TI, STG = Sh::STG, WJ = Sh::WJ;
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::body_bytes);
-
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ig = warp % WI, jg = warp / WI;
-    const int S = gridDim.y, sl = blockIdx.y;
-    const int c0 = (int)(((long long)sl * a.nchunk) / S);
-    const int c1 = (int)(((long long)(sl + 1) * a.nchunk) / S);
-    const int ntile = (c1 - c0 + TCH - 1) / TCH;
-    const int ichunk0 = (blockIdx.x * TI) / 32 + ig * NI;
-
-    double f[NI][F];
-#pragma unroll
-    for (int n = 0; n < NI; ++n)
-#pragma unroll
-        for (int c = 0; c < F; ++c) f[n][c] = 0.0;
-
-    if (tid == 0) {
-#pragma unroll
-        for (int st = 0; st < STG; ++st) mbar_init(&bar[st], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-    if (tid == 0) {
-        for (int t = 0; t < STG && t < ntile; ++t) {
-            const int cs = c0 + t * TCH, cn = min(TCH, c1 - cs);
-            const int m64 = hyb_n64<TCH, Q64>(cn), m32 = cn - m64;
-            unsigned char *dst = smem + t * Sh::tile_bytes;
-            mbar_arrive_expect_tx(&bar[t], (uint32_t)(m32 * Sh::CB32 + m64 * Sh::CB64));
-            if (m32 > 0)
-                bulk_load(dst, static_cast<const unsigned char *>(a.pred) + (size_t)cs * Sh::CB32,
-                          (uint32_t)(m32 * Sh::CB32), &bar[t]);
-            if (m64 > 0)
-                bulk_load(dst + Sh::off64,
-                          static_cast<const unsigned char *>(a.pred64) + (size_t)(cs + m32) * Sh::CB64,
-                          (uint32_t)(m64 * Sh::CB64), &bar[t]);
-        }
-    }
-
-    int failed_at;
-    if (jg >= W32) {
-        Body64 I[NI];
-#pragma unroll
-        for (int n = 0; n < NI; ++n)
-            load_i64<ORDER>(static_cast<const double *>(a.pred64), ichunk0 + n, lane, I[n]);
-        failed_at = hyb_tiles<ORDER, NW, NI, W32, W64, TCH, Q64, true, REFINE>(
-            a, smem, bar, c0, c1, ntile, jg - W32, I, f);
-    } else {
-        NegI32 I[NI];
-#pragma unroll
-        for (int n = 0; n < NI; ++n)
-            load_i_mixed<ORDER>(static_cast<const float *>(a.pred), ichunk0 + n, lane, I[n]);
-        failed_at = hyb_tiles<ORDER, NW, NI, W32, W64, TCH, Q64, false, REFINE>(
-            a, smem, bar, c0, c1, ntile, jg, I, f);
-    }
-    if (failed_at >= 0) {
-        // Leave no bulk copy writing into this CTA's shared memory after exit.
-        if (tid == 0) {
-            raise_error(a.err, kErrWaitTimeout);
-            for (int t = failed_at; t < ntile && t < failed_at + STG; ++t)
-                mbar_wait_bounded(&bar[t % STG], (uint32_t)((t / STG) & 1));
-        }
-        return;
-    }
-    force_epilogue<ORDER, NW, NI, WJ, WI, TI>(f, smem, a, ig, jg, ichunk0);
-}
 
 }  // namespace hb

@@ -6,7 +6,6 @@ namespace hb {
 
 struct ForceArgs {
     const void *pred;      // predicted slots, AoSoA32 (FP64 or mixed layout)
-    const void *pred64;    // dual-pipe mixed shapes: the same slots in the FP64 layout
     int nchunk;            // number of 32-slot j chunks (padded slots / 32)
     int nact;              // i-particles: slots [0, nact)
     double eps2;
@@ -32,8 +31,6 @@ struct ForceVariant {
     int ti;        // i per CTA
     int smem;      // dynamic shared memory bytes
     bool fused;    // predicts j (and i) from the raw records itself
-    int q64;       // dual-pipe mixed shapes: FP64 chunks per j tile (0: none);
-                   // such shapes also read the FP64 predicted layout
     void (*kern)(ForceArgs);
 };
 
@@ -135,11 +132,8 @@ cudaError_t integrator_energy(int order, const double *jp, const double *pot, in
 int force_variant_count(int order, bool mixed);
 const ForceVariant *force_variant(int order, bool mixed, int v);
 
-// pred64: with mixed, also write the FP64 layout there (the dual-pipe
-// shapes read both); nullptr otherwise.
 cudaError_t launch_predict(int order, bool mixed, const double *jp, int n, int npad,
-                           double tsys, void *pred, int *err, cudaStream_t s,
-                           void *pred64 = nullptr);
+                           double tsys, void *pred, int *err, cudaStream_t s);
 cudaError_t launch_potential(int order, const double *jp, int n, int npad, double eps2,
                              double *posm, double *pot, int *err, cudaStream_t s);
 cudaError_t run_fma_peak(int mode, int nsm, double *gflops);

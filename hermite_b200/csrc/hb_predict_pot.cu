@@ -14,12 +14,10 @@ namespace hb {
 // Slots in [n, npad) are written as zero-mass far-away padding.
 constexpr int kPredThreads = 128;
 
-// MIXED with pred64 != nullptr also writes the FP64 layout there, for the
-// dual-pipe force shapes.
 template <int ORDER, bool MIXED>
 __global__ void __launch_bounds__(kPredThreads)
 predict_kernel(const double *__restrict__ jp, int n, int npad, double tsys,
-               void *__restrict__ pred, int *err, void *__restrict__ pred64)
+               void *__restrict__ pred, int *err)
 {
     constexpr int R = Rec<ORDER>::words;
     __shared__ __align__(128) double rec[kPredThreads * R];
@@ -76,18 +74,6 @@ predict_kernel(const double *__restrict__ jp, int n, int npad, double tsys,
             if constexpr (ORDER == 8) c[(PMX_J + k) * 32] = __double2float_rn(jk[k]);
         }
         c[PMX_M * 32] = __double2float_rn(m);
-        if (pred64) {
-            constexpr int NC64 = Pred64<ORDER>::ncomp;
-            double *d = static_cast<double *>(pred64) + (size_t)ci * NC64 * 32 + lane;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                d[(P64_X + k) * 32] = x[k];
-                d[(P64_V + k) * 32] = v[k];
-                if constexpr (ORDER >= 6) d[(P64_A + k) * 32] = a[k];
-                if constexpr (ORDER >= 8) d[(P64_J + k) * 32] = jk[k];
-            }
-            d[P64_M * 32] = m;
-        }
     } else {
         constexpr int NC = Pred64<ORDER>::ncomp;
         double *c = static_cast<double *>(pred) + (size_t)ci * NC * 32 + lane;
@@ -105,25 +91,24 @@ predict_kernel(const double *__restrict__ jp, int n, int npad, double tsys,
 
 template <int ORDER, bool MIXED>
 static cudaError_t launch_predict_t(const double *jp, int n, int npad, double tsys,
-                                    void *pred, int *err, cudaStream_t s, void *pred64)
+                                    void *pred, int *err, cudaStream_t s)
 {
     const int grid = npad / kPredThreads;   // npad is a multiple of 256
-    predict_kernel<ORDER, MIXED><<<grid, kPredThreads, 0, s>>>(jp, n, npad, tsys, pred, err,
-                                                               MIXED ? pred64 : nullptr);
+    predict_kernel<ORDER, MIXED><<<grid, kPredThreads, 0, s>>>(jp, n, npad, tsys, pred, err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_predict(int order, bool mixed, const double *jp, int n, int npad,
-                           double tsys, void *pred, int *err, cudaStream_t s, void *pred64)
+                           double tsys, void *pred, int *err, cudaStream_t s)
 {
     switch (order * 2 + (mixed ? 1 : 0)) {
-    case 8:  return launch_predict_t<4, false>(jp, n, npad, tsys, pred, err, s, pred64);
-    case 9:  return launch_predict_t<4, true>(jp, n, npad, tsys, pred, err, s, pred64);
-    case 12: return launch_predict_t<6, false>(jp, n, npad, tsys, pred, err, s, pred64);
-    case 13: return launch_predict_t<6, true>(jp, n, npad, tsys, pred, err, s, pred64);
-    case 16: return launch_predict_t<8, false>(jp, n, npad, tsys, pred, err, s, pred64);
-    case 17: return launch_predict_t<8, true>(jp, n, npad, tsys, pred, err, s, pred64);
-    case 18: return launch_predict_t<9, false>(jp, n, npad, tsys, pred, err, s, pred64);
+    case 8:  return launch_predict_t<4, false>(jp, n, npad, tsys, pred, err, s);
+    case 9:  return launch_predict_t<4, true>(jp, n, npad, tsys, pred, err, s);
+    case 12: return launch_predict_t<6, false>(jp, n, npad, tsys, pred, err, s);
+    case 13: return launch_predict_t<6, true>(jp, n, npad, tsys, pred, err, s);
+    case 16: return launch_predict_t<8, false>(jp, n, npad, tsys, pred, err, s);
+    case 17: return launch_predict_t<8, true>(jp, n, npad, tsys, pred, err, s);
+    case 18: return launch_predict_t<9, false>(jp, n, npad, tsys, pred, err, s);
     }
     return cudaErrorInvalidValue;
 }

@@ -72,47 +72,6 @@ def test_every_launch_shape(precision, variant, jsplit, oracle):
     _check(6, 2500, 700, precision, oracle, seed=11, variant=variant, jsplit=jsplit)
 
 
-# Mixed precision on both pipes: i-groups of mixed-precision and FP64 warps
-# sharing every j tile (force_kernel_hyb); N and nact not multiples of a tile,
-# so partial tiles split their chunks between the precisions too.
-HYB_VARIANTS = [20, 21, 22, 23]
-
-
-@pytest.mark.parametrize("order", [4, 6, 8])
-@pytest.mark.parametrize("variant", HYB_VARIANTS)
-@pytest.mark.parametrize("jsplit", [1, 3, 16])
-def test_dual_pipe_shapes(order, variant, jsplit, oracle):
-    _check(order, 2500, 700, "mixed", oracle, seed=11 + order, variant=variant, jsplit=jsplit)
-
-
-@pytest.mark.parametrize("variant", HYB_VARIANTS)
-def test_dual_pipe_small_and_full(variant, oracle):
-    for n, nact in ((1, 1), (33, 33), (4097, 4097), (5000, 130)):
-        _check(6, n, nact, "mixed", oracle, seed=n, variant=variant)
-
-
-def test_dual_pipe_after_single_pipe_shape(oracle):
-    """One predict_all, then a single-pipe and a dual-pipe launch: the second
-    needs the FP64 layout the first did not write, so the predictor runs
-    again; both match the oracle."""
-    order, n, nact = 6, 3000, 500
-    rec = make_records(order, n, seed=21)
-    ref = oracle.predict_force(order, rec, 0.0, nact, EPS2)
-    with Gravity(order, n, "mixed") as g:
-        g.set_jp_records(rec)
-        g.predict_all(0.0)
-        g.set_force_shape(0, 4)
-        a = g.calc_force_on_first_nact(nact, EPS2)
-        g.set_force_shape(20, 4)
-        b = g.calc_force_on_first_nact(nact, EPS2)
-        g.set_force_shape(1, 2)
-        c = g.calc_force_on_first_nact(nact, EPS2)
-    for got in (a, b, c):
-        err = rel_err(got, ref)
-        for k in range(err.shape[1]):
-            assert err[:, k].max() <= MIXED_TOL[k]
-
-
 @pytest.mark.parametrize("order", [4, 6, 8])
 def test_potential(order, oracle):
     n = 1500
@@ -138,26 +97,6 @@ def test_self_term_is_zero(variant):
                 g.predict_all(0.0)
                 f = g.calc_force_on_first_nact(1, EPS2)
             assert np.all(f == 0.0), (order, prec, variant)
-
-
-def test_self_term_is_zero_dual_pipe():
-    """The self pair adds exactly zero whether it lands in a mixed-precision
-    or an FP64 chunk of a dual-pipe tile.  240 slots (8 chunks after padding,
-    one tile at one slice, split 7:1 by shape 21): only slot 10 (chunk 0,
-    mixed) or slot 230 (chunk 7, FP64) has mass, so the force on it is its
-    self term alone."""
-    for order in (4, 6, 8):
-        for heavy in (10, 230):
-            rec = make_records(order, 240, seed=2)
-            rec[:, 3] = 0.0
-            rec[heavy, 3] = 1.0 / 240
-            with Gravity(order, 240, "mixed") as g:
-                g.set_force_shape(21, 1)
-                g.set_jp_records(rec)
-                g.predict_all(0.0)
-                f = g.calc_force_on_first_nact(240, EPS2)
-            assert np.all(f[heavy] == 0.0), (order, heavy)
-            assert np.all(np.isfinite(f))
 
 
 @pytest.mark.parametrize("order", [4, 6, 8])

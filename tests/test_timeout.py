@@ -24,7 +24,6 @@ TOL = {"fp64": 1e-12, "mixed": 1e-5}
     (6, "mixed", 1, 4),    # 2 i-chunks per warp, four j-slices
     (8, "fp64", 2, 8),     # four warps split every tile, eight j-slices
     (4, "fp64", 12, 2),    # fused predict + force: the i-record wait gives up
-    (6, "mixed", 20, 4),   # mixed precision on both pipes: two copies per tile
 ])
 def test_wait_timeout_reported_and_context_recovers(order, precision, variant, jsplit, oracle):
     n, nact = 4096, 1000
