@@ -723,8 +723,9 @@ def device_integrator_leg(configs=("c1", "c2", "c3")):
     (N = 1024) runs on both engines: "team" (one thread-block cluster, the
     whole loop in one kernel; the automatic choice at this N) and "graph"
     (four kernels per step over the whole GPU, 32 steps per CUDA-graph
-    replay; the automatic choice for c2 and c3).  c2 and c3 run windows
-    (t = 0..1/64 and 0..1/32)."""
+    replay; the automatic choice for c2 and c3) and "persistent" (the same
+    phases in one cooperative kernel, grid barriers between them).  c2 and c3
+    run windows (t = 0..1/64 and 0..1/32)."""
     from hermite_b200 import Gravity
     from hermite_b200.ic import plummer, records
     from run_app import CONFIGS
@@ -736,7 +737,7 @@ def device_integrator_leg(configs=("c1", "c2", "c3")):
             cfg["tend"] = 1.0 / 64 if name == "c2" else 1.0 / 32
         order, n = cfg["order"], cfg["n"]
         eps2 = cfg["eps"] ** 2
-        engines = ("team", "graph") if name == "c1" else ("auto",)
+        engines = ("team", "graph", "persistent") if name == "c1" else ("graph", "persistent")
         for eng in engines:
             prec = "fp64"
             with Gravity(order, n, prec) as g:
@@ -751,7 +752,7 @@ def device_integrator_leg(configs=("c1", "c2", "c3")):
                 ps, bs, t = g.integrator_stats()
                 ke, pe = g.energy(eps2)
             e0 = ke0 + pe0
-            key = f"{name}_{prec}" if eng != "graph" else f"{name}_{prec}_graph"
+            key = f"{name}_{prec}_{used[0]}"
             out[key] = {
                 "engine": used[0], "team_ctas": used[1],
                 "order": order, "n": n, "tend": cfg["tend"], "block_steps": bs,

@@ -58,7 +58,7 @@ EXPORTED_SYMBOLS = (
 )
 
 
-ENGINES = {"auto": 0, "graph": 1, "team": 2}
+ENGINES = {"auto": 0, "graph": 1, "team": 2, "persistent": 3}
 
 
 def record_words(order: int) -> int:
@@ -367,8 +367,10 @@ class Gravity:
                      "integrator_run")
 
     def set_engine(self, engine: str = "auto", team_ctas: int = 0):
-        """Integration engine: "auto", "graph" (multi-kernel, CUDA graph) or
-        "team" (one thread-block cluster, whole loop in one kernel)."""
+        """Integration engine: "auto", "graph" (multi-kernel, CUDA graph),
+        "team" (one thread-block cluster, whole loop in one kernel) or
+        "persistent" (one cooperative kernel over the whole GPU, grid
+        barriers between the phases of a step)."""
         self._check(self._lib.hb_integrator_set_engine(self._h, ENGINES[engine], int(team_ctas)),
                     "set_engine")
 

@@ -91,6 +91,10 @@ struct hb_ctx {
     double *d_aux = nullptr;          // per-slot dump derivatives
     TeamState *d_team_state = nullptr;
     int *d_team_next = nullptr;
+    // persistent engine
+    unsigned *d_gbar = nullptr;       // grid barrier words, zero between launches
+    IntegratorLaunch int_L{};         // the step's buffers and work-item target
+    int persist_grid = 0;             // resident CTAs of the persistent kernel
     int blocks_per_sm[2][kNumVariants] = {};
     bool smem_set[2][kNumVariants] = {};
     std::string err;
@@ -366,6 +370,7 @@ int hb_destroy(hb_ctx *ctx)
     cudaFree(ctx->d_aux);
     cudaFree(ctx->d_team_state);
     cudaFree(ctx->d_team_next);
+    cudaFree(ctx->d_gbar);
     if (ctx->ev_upload) cudaEventDestroy(ctx->ev_upload);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -698,7 +703,9 @@ int integrator_alloc(hb_ctx *ctx)
               cudaMalloc((void **)&ctx->d_aux, np * kAuxWords * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_team_sys, sizeof(TeamSys)) == cudaSuccess &&
               cudaMalloc((void **)&ctx->d_team_state, sizeof(TeamState)) == cudaSuccess &&
-              cudaMalloc((void **)&ctx->d_team_next, sizeof(int)) == cudaSuccess;
+              cudaMalloc((void **)&ctx->d_team_next, sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&ctx->d_gbar, 2 * sizeof(unsigned)) == cudaSuccess &&
+              cudaMemset(ctx->d_gbar, 0, 2 * sizeof(unsigned)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         return fail(ctx, HB_ERR_ALLOC, "integrator buffers could not be allocated");
@@ -755,6 +762,10 @@ int setup_integrator(hb_ctx *ctx, double tsys, double eps2, double eta, double d
     L.items_grid = ctx->nsm * std::max(1, per_sm);
     L.big_grid = ctx->nsm * std::max(1, big_per_sm);
     L.target_items = 2 * L.items_grid;
+    ctx->int_L = L;
+    int psmem = 0, p_per_sm = 0;
+    HB_CK(persistent_setup(ctx->order, L.mixed, &psmem, &p_per_sm));
+    ctx->persist_grid = ctx->nsm * p_per_sm;
 
     if (ctx->stream == nullptr) return fail(ctx, HB_ERR_STATE, "integrator needs a non-default stream");
     HB_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -920,6 +931,7 @@ int team_config_for(hb_ctx *ctx, int n, int want_ctas, TeamConfig *cfg)
 int resolve_engine(hb_ctx *ctx, TeamConfig *cfg)
 {
     if (ctx->engine == HB_ENGINE_GRAPH) return HB_ENGINE_GRAPH;
+    if (ctx->engine == HB_ENGINE_PERSISTENT) return HB_ENGINE_PERSISTENT;
     const bool fp64 = ctx->precision == HB_FP64;
     if (ctx->engine == HB_ENGINE_TEAM) {
         if (!fp64) return -fail(ctx, HB_ERR_INVALID, "the team engine integrates in FP64 only");
@@ -973,11 +985,52 @@ int run_team(hb_ctx *ctx, const TeamConfig &cfg, double tend, long long max_bloc
     }
     return HB_OK;
 }
+
+// The persistent engine: one cooperative launch per kPersistStepsPerLaunch
+// block steps; the host reads the mapped status between launches.
+constexpr long long kPersistStepsPerLaunch = 4096;
+
+int run_persistent(hb_ctx *ctx, double tend, long long max_block_steps)
+{
+    if (ctx->persist_grid <= 0)
+        return fail(ctx, HB_ERR_CUDA, "the persistent kernel cannot be resident on this device");
+    volatile IntStatus *st = ctx->h_status;
+    const long long first_steps = st->block_steps;
+    long long last_steps = st->block_steps;
+    while (st->tsys < tend) {
+        long long budget = kPersistStepsPerLaunch;
+        if (max_block_steps > 0) {
+            const long long left = max_block_steps - (st->block_steps - first_steps);
+            if (left <= 0)
+                return fail(ctx, HB_ERR_STATE, "block-step limit %lld reached at t = %.17g",
+                            max_block_steps, st->tsys);
+            budget = std::min(budget, left);
+        }
+        HB_CK(persistent_launch(ctx->order, ctx->int_L, ctx->d_gbar, budget, ctx->wait_limit,
+                                ctx->persist_grid, ctx->stream));
+        ctx->launches += 1;
+        const int s = sync_stream(ctx);
+        if (s != HB_OK) {
+            // a barrier or tile wait gave up: the barrier words are left mid-use
+            cudaMemsetAsync(ctx->d_gbar, 0, 2 * sizeof(unsigned), ctx->stream);
+            cudaStreamSynchronize(ctx->stream);
+            return s;
+        }
+        if (st->error)
+            return fail(ctx, st->error == 2 ? HB_ERR_DEVICE_TIMEOUT : HB_ERR_STATE,
+                        st->error == 2 ? "a device-side wait gave up" : "a timestep underflowed (< 2^-48)");
+        if (st->block_steps == last_steps && st->tsys < tend)
+            return fail(ctx, HB_ERR_STATE, "integration stalled at t = %.17g", st->tsys);
+        last_steps = st->block_steps;
+    }
+    return HB_OK;
+}
 }  // namespace
 
 int hb_integrator_set_engine(hb_ctx *ctx, int engine, int team_ctas)
 {
-    if (!ctx || engine < HB_ENGINE_AUTO || engine > HB_ENGINE_TEAM || team_ctas < 0 || team_ctas > 16)
+    if (!ctx || engine < HB_ENGINE_AUTO || engine > HB_ENGINE_PERSISTENT || team_ctas < 0 ||
+        team_ctas > 16)
         return HB_ERR_INVALID;
     ctx->engine = engine;
     ctx->team_ctas = team_ctas;
@@ -1008,6 +1061,7 @@ int hb_integrator_run(hb_ctx *ctx, double tend, long long max_block_steps)
     const int engine = resolve_engine(ctx, &cfg);
     if (engine < 0) return -engine;
     if (engine == HB_ENGINE_TEAM) return run_team(ctx, cfg, tend, max_block_steps);
+    if (engine == HB_ENGINE_PERSISTENT) return run_persistent(ctx, tend, max_block_steps);
     long long last_steps = st->block_steps;
     const long long first_steps = st->block_steps;
     while (st->tsys < tend) {

@@ -55,10 +55,9 @@ __device__ __forceinline__ void pdl_enter()
 
 // ---------------------------------------------------------------------------
 template <int ORDER>
-__global__ void sched_min_kernel(const double *__restrict__ jp, const double *__restrict__ dt,
-                                 int n, Sched *s)
+__device__ __forceinline__ void min_phase(const double *__restrict__ jp, const double *__restrict__ dt,
+                                          int n, Sched *s)
 {
-    pdl_enter();
     constexpr int R = Rec<ORDER>::words;
     double m = __longlong_as_double((long long)kInfBits);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -78,12 +77,22 @@ __global__ void sched_min_kernel(const double *__restrict__ jp, const double *__
     }
 }
 
-// Active set and dtlim.  Positive doubles order like their bit patterns.
 template <int ORDER>
-__global__ void sched_compact_kernel(const double *__restrict__ jp, const double *__restrict__ dt,
-                                     int n, Sched *s, int *__restrict__ ilist)
+__global__ void sched_min_kernel(const double *__restrict__ jp, const double *__restrict__ dt,
+                                 int n, Sched *s)
 {
     pdl_enter();
+    min_phase<ORDER>(jp, dt, n, s);
+}
+
+// Active set and dtlim.  Positive doubles order like their bit patterns.
+// Returns whether the step is live (tnext within tend and no error): the same
+// answer in every thread of the grid.
+template <int ORDER>
+__device__ __forceinline__ bool compact_phase(const double *__restrict__ jp,
+                                              const double *__restrict__ dt, int n, Sched *s,
+                                              int *__restrict__ ilist)
+{
     constexpr int R = Rec<ORDER>::words;
     const double tnext = __longlong_as_double((long long)s->tnext_bits);
     const bool live = tnext <= s->tend && s->error == 0;
@@ -98,7 +107,7 @@ __global__ void sched_compact_kernel(const double *__restrict__ jp, const double
         s->tnext = tnext;
         s->dtlim = dtlim;
     }
-    if (!live) return;
+    if (!live) return false;
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const int i = base + threadIdx.x;
         const bool act = i < n && dt[i] + jp[(size_t)i * R + 7] == tnext;
@@ -108,6 +117,15 @@ __global__ void sched_compact_kernel(const double *__restrict__ jp, const double
         off = __shfl_sync(0xffffffffu, off, 0);
         if (act) ilist[off + __popc(ballot & ((1u << (threadIdx.x & 31)) - 1u))] = i;
     }
+    return true;
+}
+
+template <int ORDER>
+__global__ void sched_compact_kernel(const double *__restrict__ jp, const double *__restrict__ dt,
+                                     int n, Sched *s, int *__restrict__ ilist)
+{
+    pdl_enter();
+    compact_phase<ORDER>(jp, dt, n, s, ilist);
 }
 
 // Sum of the S slice partials of one i-tile (V values, slice stride sstride
@@ -168,22 +186,26 @@ struct ItemsArgs {
 };
 
 template <int ORDER, bool MIXED>
-__global__ void __launch_bounds__(128)
-force_items_kernel(ItemsArgs a)
+using ItemsShape = ForceShape<ORDER, MIXED, 4, 1, 4, 4, true>;
+
+// The work items of one step with 1..big_nact active slots, taken by this CTA
+// until none are left.  smem: ItemsShape's layout; bar: two initialised
+// mbarriers whose phases continue from g (tiles issued by this CTA before).
+// Returns false when a wait gave up (the error is raised, the CTA's copies
+// drained).
+template <int ORDER, bool MIXED>
+__device__ __forceinline__ bool items_phase(const ItemsArgs &a, unsigned char *smem, uint64_t *bar,
+                                            unsigned &g)
 {
-    pdl_enter();
     constexpr int NW = 4, WJ = 4, TCH = 4, STG = 2, TI = 32;
     constexpr int F = Frc<ORDER>::words, R = Rec<ORDER>::words, RB = Rec<ORDER>::bytes;
-    using Sh = ForceShape<ORDER, MIXED, NW, 1, WJ, TCH, true>;
+    using Sh = ItemsShape<ORDER, MIXED>;
     constexpr int CB = Sh::CB;
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::body_bytes);
     unsigned char *ptile = smem + Sh::ring_bytes;
     __shared__ int s_item;
     __shared__ unsigned s_last;
 
     const int nact = a.s->nact;
-    if (nact == 0 || nact > a.big_nact) return;   // large steps: force_items_big_kernel
     const double tsys = a.s->tnext, eps2 = a.s->eps2;
     const int tid = threadIdx.x, lane = tid & 31, jg = tid >> 5;
     const int gx = (nact + TI - 1) / TI;
@@ -194,14 +216,6 @@ force_items_kernel(ItemsArgs a)
     const int items = gx * S;
     const size_t ispan = (size_t)gx * TI;
 
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    unsigned g = 0;   // tiles issued by this CTA so far (mbarrier phases)
     const float2 eps2f = f2((float)eps2);
     for (;;) {
         if (tid == 0) s_item = atomicAdd(&a.s->work, 1);
@@ -268,7 +282,7 @@ force_items_kernel(ItemsArgs a)
                     mbar_wait_bounded(&bar[(g + t) % STG], ((g + t) / STG) & 1u);
             }
             a.s->error = 2;
-            return;
+            return false;
         }
         g += ntile;
 
@@ -307,6 +321,27 @@ force_items_kernel(ItemsArgs a)
         }
         __syncthreads();
     }
+    return true;
+}
+
+template <int ORDER, bool MIXED>
+__global__ void __launch_bounds__(128)
+force_items_kernel(ItemsArgs a)
+{
+    pdl_enter();
+    using Sh = ItemsShape<ORDER, MIXED>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + Sh::body_bytes);
+    const int nact = a.s->nact;
+    if (nact == 0 || nact > a.big_nact) return;   // large steps: force_items_big_kernel
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned g = 0;   // tiles issued by this CTA so far (mbarrier phases)
+    items_phase<ORDER, MIXED>(a, smem, bar, g);
 }
 
 // The same work for steps with many active slots: items of 4 warps x NI
@@ -324,22 +359,19 @@ struct BigShape {
     static_assert(TI * RB <= ring_bytes, "the raw i-tile must fit the ring");
 };
 
+// Large-step counterpart of items_phase (smem: BigShape's layout).
 template <int ORDER, bool MIXED>
-__global__ void __launch_bounds__(128)
-force_items_big_kernel(ItemsArgs a)
+__device__ __forceinline__ bool big_phase(const ItemsArgs &a, unsigned char *smem, uint64_t *bar,
+                                          unsigned &g)
 {
-    pdl_enter();
     using B = BigShape<ORDER, MIXED>;
     constexpr int NW = B::NW, NI = B::NI, TCH = B::TCH, STG = B::STG, TI = B::TI, CB = B::CB;
     constexpr int F = Frc<ORDER>::words, R = Rec<ORDER>::words, RB = Rec<ORDER>::bytes;
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + B::ring_bytes + B::ptile_bytes);
     unsigned char *ptile = smem + B::ring_bytes;
     __shared__ int s_item;
     __shared__ unsigned s_last;
 
     const int nact = a.s->nact;
-    if (nact <= a.big_nact) return;
     const double tsys = a.s->tnext, eps2 = a.s->eps2;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int gx = (nact + TI - 1) / TI;
@@ -349,14 +381,6 @@ force_items_big_kernel(ItemsArgs a)
     const int items = gx * S;
     const size_t ispan = (size_t)gx * TI;
 
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    unsigned g = 0;   // tiles issued by this CTA so far (mbarrier phases)
     const float2 eps2f = f2((float)eps2);
     for (;;) {
         if (tid == 0) s_item = atomicAdd(&a.s->work, 1);
@@ -428,7 +452,7 @@ force_items_big_kernel(ItemsArgs a)
                     mbar_wait_bounded(&bar[(g + t) % STG], ((g + t) / STG) & 1u);
             }
             a.s->error = 2;
-            return;
+            return false;
         }
         g += ntile;
 
@@ -461,14 +485,34 @@ force_items_big_kernel(ItemsArgs a)
         }
         __syncthreads();
     }
+    return true;
+}
+
+template <int ORDER, bool MIXED>
+__global__ void __launch_bounds__(128)
+force_items_big_kernel(ItemsArgs a)
+{
+    pdl_enter();
+    using B = BigShape<ORDER, MIXED>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + B::ring_bytes + B::ptile_bytes);
+    if (a.s->nact <= a.big_nact) return;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned g = 0;   // tiles issued by this CTA so far (mbarrier phases)
+    big_phase<ORDER, MIXED>(a, smem, bar, g);
 }
 
 template <int ORDER>
-__global__ void correct_kernel(double *__restrict__ jp, double *__restrict__ dt,
-                               const double *__restrict__ force, const int *__restrict__ ilist,
-                               Sched *s, double *__restrict__ aux)
+__device__ __forceinline__ void correct_phase(double *__restrict__ jp, double *__restrict__ dt,
+                                              const double *__restrict__ force,
+                                              const int *__restrict__ ilist, Sched *s,
+                                              double *__restrict__ aux)
 {
-    pdl_enter();
     constexpr int R = Rec<ORDER>::words, F = Frc<ORDER>::words;
     const int nact = s->nact;
     const double dtlim = s->dtlim, etapow = s->etapow;
@@ -491,6 +535,116 @@ __global__ void correct_kernel(double *__restrict__ jp, double *__restrict__ dt,
         st->particle_steps = s->particle_steps;
         st->block_steps = s->block_steps;
         st->error = s->error;
+    }
+}
+
+template <int ORDER>
+__global__ void correct_kernel(double *__restrict__ jp, double *__restrict__ dt,
+                               const double *__restrict__ force, const int *__restrict__ ilist,
+                               Sched *s, double *__restrict__ aux)
+{
+    pdl_enter();
+    correct_phase<ORDER>(jp, dt, force, ilist, s, aux);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent engine: the four phases of a block step (next block time, active
+// set, force, corrector) in one cooperative kernel, its CTAs all resident,
+// separated by grid barriers in place of kernel boundaries; up to max_steps
+// steps per launch.  The phases are the graph engine's own code, and the
+// force phases take the same work items (same target), so both engines give
+// the same block steps and records bit for bit.
+struct PersistArgs {
+    ItemsArgs it;
+    int *ilist;              // writable views of it.ilist and it.jp
+    double *jp;
+    double *dt, *aux;
+    unsigned *gbar;          // grid barrier: [0] arrivals, [1] generation
+    long long max_steps;
+    unsigned spin;           // poll limit of one barrier wait
+};
+
+template <int ORDER, bool MIXED>
+struct PersistSmem {
+    static constexpr int items = ItemsShape<ORDER, MIXED>::body_bytes;
+    static constexpr int big = BigShape<ORDER, MIXED>::ring_bytes + BigShape<ORDER, MIXED>::ptile_bytes;
+    static constexpr int bar_off = ((items > big ? items : big) + 15) / 16 * 16;
+    static constexpr int bytes = bar_off + 64;
+};
+
+// Barrier over a co-resident grid.  Thread 0 of each CTA reads the generation
+// word, arrives on the counter; the last CTA to arrive resets the counter and
+// advances the generation, which the others poll.  Fences on both sides make
+// the writes before the barrier visible after it.  A wait is bounded: after
+// `spin` polls the CTA reports false (the caller raises the error and
+// returns; the other CTAs then give up at their next barrier).
+__device__ __forceinline__ bool grid_barrier(unsigned *gbar, unsigned spin)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = gbar + 1;
+        const unsigned my = *gen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(gbar, 1u) == gridDim.x - 1) {
+            atomicExch(gbar, 0u);
+            __threadfence();
+            atomicAdd(gbar + 1, 1u);
+        } else {
+            ok = 0;
+            for (unsigned it = 0; it < spin; ++it) {
+                if (*gen != my) {
+                    ok = 1;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <int ORDER, bool MIXED>
+__global__ void __launch_bounds__(128)
+persistent_kernel(PersistArgs p)
+{
+    using P = PersistSmem<ORDER, MIXED>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + P::bar_off);
+    const ItemsArgs &a = p.it;
+    Sched *s = a.s;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned g = 0;   // tiles issued by this CTA so far (mbarrier phases)
+    for (long long k = 0; k < p.max_steps; ++k) {
+        min_phase<ORDER>(a.jp, p.dt, a.n, s);
+        if (!grid_barrier(p.gbar, p.spin)) break;
+        const bool live = compact_phase<ORDER>(a.jp, p.dt, a.n, s, p.ilist);
+        if (!grid_barrier(p.gbar, p.spin)) break;
+        if (!live) return;               // every CTA reads the same state
+        const int nact = s->nact;
+        if (nact > 0) {
+            const bool ok = nact <= a.big_nact ? items_phase<ORDER, MIXED>(a, smem, bar, g)
+                                               : big_phase<ORDER, MIXED>(a, smem, bar, g);
+            if (!ok) return;             // raised; the others give up at the next barrier
+        }
+        if (!grid_barrier(p.gbar, p.spin)) break;
+        correct_phase<ORDER>(p.jp, p.dt, a.force, a.ilist, s, p.aux);
+        if (!grid_barrier(p.gbar, p.spin)) break;
+        if (k + 1 == p.max_steps) return;
+    }
+    // a barrier wait gave up
+    if (threadIdx.x == 0) {
+        s->error = 2;
+        raise_error(a.err, kErrWaitTimeout);
     }
 }
 
@@ -665,6 +819,65 @@ cudaError_t integrator_kernel_setup(int order, bool mixed, int *smem, int *grid_
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(big_per_sm, k, 128, sm);
+}
+
+template <int ORDER, bool MIXED>
+static cudaError_t persistent_setup_t(int *smem, int *per_sm)
+{
+    const void *k = (const void *)&persistent_kernel<ORDER, MIXED>;
+    *smem = PersistSmem<ORDER, MIXED>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, 128, *smem);
+    return e;
+}
+
+cudaError_t persistent_setup(int order, bool mixed, int *smem, int *per_sm)
+{
+    switch (order * 2 + (mixed ? 1 : 0)) {
+    case 8: return persistent_setup_t<4, false>(smem, per_sm);
+    case 9: return persistent_setup_t<4, true>(smem, per_sm);
+    case 12: return persistent_setup_t<6, false>(smem, per_sm);
+    case 13: return persistent_setup_t<6, true>(smem, per_sm);
+    case 16: return persistent_setup_t<8, false>(smem, per_sm);
+    case 17: return persistent_setup_t<8, true>(smem, per_sm);
+    case 18: return persistent_setup_t<9, false>(smem, per_sm);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int ORDER, bool MIXED>
+static cudaError_t persistent_launch_t(const PersistArgs &p, int grid, cudaStream_t s)
+{
+    PersistArgs arg = p;
+    void *args[] = {&arg};
+    return cudaLaunchCooperativeKernel((const void *)&persistent_kernel<ORDER, MIXED>, dim3(grid),
+                                       dim3(128), args, (size_t)PersistSmem<ORDER, MIXED>::bytes, s);
+}
+
+cudaError_t persistent_launch(int order, const IntegratorLaunch &L, unsigned *gbar,
+                              long long max_steps, unsigned spin, int grid, cudaStream_t s)
+{
+    PersistArgs p;
+    p.it = ItemsArgs{L.jp, L.ilist, L.sched, L.force, L.partial, L.counter, L.err, L.n, L.nchunk,
+                     L.partial_cap, L.target_items, kBigNact};
+    p.ilist = L.ilist;
+    p.jp = L.jp;
+    p.dt = L.dt;
+    p.aux = L.aux;
+    p.gbar = gbar;
+    p.max_steps = max_steps;
+    p.spin = spin;
+    const bool mixed = L.mixed && order != 9;
+    switch (order * 2 + (mixed ? 1 : 0)) {
+    case 8: return persistent_launch_t<4, false>(p, grid, s);
+    case 9: return persistent_launch_t<4, true>(p, grid, s);
+    case 12: return persistent_launch_t<6, false>(p, grid, s);
+    case 13: return persistent_launch_t<6, true>(p, grid, s);
+    case 16: return persistent_launch_t<8, false>(p, grid, s);
+    case 17: return persistent_launch_t<8, true>(p, grid, s);
+    case 18: return persistent_launch_t<9, false>(p, grid, s);
+    }
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t integrator_assign(int order, double *jp, double *dt, const double *force, int n,

@@ -80,6 +80,14 @@ struct IntegratorLaunch {
 
 cudaError_t integrator_step_launch(int order, const IntegratorLaunch &L, cudaStream_t s);
 
+// Persistent engine (hb_integrator.cu): one cooperative launch runs up to
+// max_steps block steps; gbar is two zeroed words (grid barrier); spin is the
+// poll limit of a barrier wait.  setup: dynamic shared memory and resident
+// CTAs per SM of the kernel.
+cudaError_t persistent_setup(int order, bool mixed, int *smem, int *per_sm);
+cudaError_t persistent_launch(int order, const IntegratorLaunch &L, unsigned *gbar,
+                              long long max_steps, unsigned spin, int grid, cudaStream_t s);
+
 // Team engine (hb_team.cu): one thread-block cluster of `ctas` CTAs runs the
 // whole block-step loop of one system at a time inside one kernel.
 constexpr int kTeamIMax = 256;              // smallest round of i-states

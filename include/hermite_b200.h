@@ -145,7 +145,8 @@ int hb_synchronize(hb_ctx *ctx);
 long long hb_launch_count(const hb_ctx *ctx);
 
 /* Test hook: the poll limit of the force kernel's waits for incoming j tiles
- * (default and maximum 1<<22 polls; polls < 0 restores the default).  A
+ * (default and maximum 1<<22 polls; polls < 0 restores the default), and of
+ * the persistent engine's grid-barrier waits.  A
  * limit of 0 makes every such wait give up at once, so a test can drive the
  * kernel's timeout path with no fault: the kernel raises its error flag, its
  * waits for the copies already in flight keep the full limit, the call
@@ -185,6 +186,11 @@ int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double
 /* Engines for hb_integrator_run (same state, same algorithm):
  *  HB_ENGINE_GRAPH  four kernels per block step over the whole GPU, 32 steps
  *                   per replay of a CUDA graph (any N, FP64 or mixed);
+ *  HB_ENGINE_PERSISTENT  the graph engine's phases in one cooperative kernel
+ *                   whose CTAs all stay resident, grid barriers (bounded
+ *                   waits) between the phases, up to 4096 block steps per
+ *                   launch; the same block steps and records as the graph
+ *                   engine, bit for bit (any N, FP64 or mixed);
  *  HB_ENGINE_TEAM   one thread-block cluster of up to 16 CTAs runs the whole
  *                   block-step loop in one kernel, three cluster barriers per
  *                   step (FP64; N up to 16 x the slots one CTA holds in
@@ -192,9 +198,9 @@ int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double
  *  HB_ENGINE_AUTO   the team engine for FP64 systems of up to 3072
  *                   particles, else the graph engine (the default).
  * team_ctas: CTAs per team (1..16), 0 = chosen from N. */
-enum { HB_ENGINE_AUTO = 0, HB_ENGINE_GRAPH = 1, HB_ENGINE_TEAM = 2 };
+enum { HB_ENGINE_AUTO = 0, HB_ENGINE_GRAPH = 1, HB_ENGINE_TEAM = 2, HB_ENGINE_PERSISTENT = 3 };
 int hb_integrator_set_engine(hb_ctx *ctx, int engine, int team_ctas);
-/* The engine (HB_ENGINE_GRAPH or HB_ENGINE_TEAM) and team size the next
+/* The engine (HB_ENGINE_GRAPH, _TEAM or _PERSISTENT) and team size the next
  * hb_integrator_run uses; HB_ERR_TOO_LARGE / HB_ERR_INVALID when a forced
  * team engine cannot take this system. */
 int hb_integrator_engine(hb_ctx *ctx, int *engine, int *team_ctas);

@@ -27,7 +27,7 @@ def _snapshot(tmp_path, nk):
     return read_snapshot(tmp_path / f"pl{nk}k.dat")
 
 
-@pytest.mark.parametrize("engine", ["graph", "team"])
+@pytest.mark.parametrize("engine", ["graph", "team", "persistent"])
 @pytest.mark.parametrize("order,nk", [(4, 1), (6, 1), (8, 1), (4, 2), (6, 2)])
 def test_device_integrator_nact_known_answer(order, nk, engine, tmp_path):
     from hermite_b200 import Gravity
