@@ -573,35 +573,50 @@ struct PersistSmem {
 };
 
 // Barrier over a co-resident grid.  Thread 0 of each CTA reads the generation
-// word, arrives on the counter; the last CTA to arrive resets the counter and
-// advances the generation, which the others poll.  Fences on both sides make
-// the writes before the barrier visible after it.  A wait is bounded: after
-// `spin` polls the CTA reports false (the caller raises the error and
-// returns; the other CTAs then give up at their next barrier).
+// word, then arrives on the counter (acquire-release); the last CTA to arrive
+// resets the counter and advances the generation (release), which the others
+// poll (acquire).  The CTA barriers on both sides carry the ordering to the
+// CTA's other threads, so every write made before the barrier anywhere in the
+// grid is visible to every read after it (the acquire also drops stale L1
+// lines).  A wait is bounded: after `spin` polls the CTA reports false (the
+// caller raises the error and returns; the other CTAs then give up at their
+// next barrier).
+__device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ bool grid_barrier(unsigned *gbar, unsigned spin)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *gen = gbar + 1;
-        const unsigned my = *gen;
-        __threadfence();
+        const unsigned my = ld_relaxed_gpu(gbar + 1);
+        unsigned old;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;"
+                     : "=r"(old) : "l"(gbar) : "memory");
         int ok = 1;
-        if (atomicAdd(gbar, 1u) == gridDim.x - 1) {
-            atomicExch(gbar, 0u);
-            __threadfence();
-            atomicAdd(gbar + 1, 1u);
+        if (old == gridDim.x - 1) {
+            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" :: "l"(gbar) : "memory");
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" :: "l"(gbar + 1) : "memory");
         } else {
             ok = 0;
             for (unsigned it = 0; it < spin; ++it) {
-                if (*gen != my) {
+                if (ld_acquire_gpu(gbar + 1) != my) {
                     ok = 1;
                     break;
                 }
                 __nanosleep(64);
             }
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
@@ -624,25 +639,28 @@ persistent_kernel(PersistArgs p)
     }
     __syncthreads();
     unsigned g = 0;   // tiles issued by this CTA so far (mbarrier phases)
-    for (long long k = 0; k < p.max_steps; ++k) {
+    bool gave_up = false;
+    for (long long k = 0; k < p.max_steps && !gave_up; ++k) {
         min_phase<ORDER>(a.jp, p.dt, a.n, s);
-        if (!grid_barrier(p.gbar, p.spin)) break;
+        if (!grid_barrier(p.gbar, p.spin)) { gave_up = true; break; }
         const bool live = compact_phase<ORDER>(a.jp, p.dt, a.n, s, p.ilist);
-        if (!grid_barrier(p.gbar, p.spin)) break;
-        if (!live) return;               // every CTA reads the same state
+        if (!grid_barrier(p.gbar, p.spin)) { gave_up = true; break; }
+        if (!live) {                     // every CTA reads the same state
+            // as the graph engine leaves a step past tend
+            if (blockIdx.x == 0 && threadIdx.x == 0) s->tnext_bits = kInfBits;
+            return;
+        }
         const int nact = s->nact;
         if (nact > 0) {
             const bool ok = nact <= a.big_nact ? items_phase<ORDER, MIXED>(a, smem, bar, g)
                                                : big_phase<ORDER, MIXED>(a, smem, bar, g);
             if (!ok) return;             // raised; the others give up at the next barrier
         }
-        if (!grid_barrier(p.gbar, p.spin)) break;
+        if (!grid_barrier(p.gbar, p.spin)) { gave_up = true; break; }
         correct_phase<ORDER>(p.jp, p.dt, a.force, a.ilist, s, p.aux);
-        if (!grid_barrier(p.gbar, p.spin)) break;
-        if (k + 1 == p.max_steps) return;
+        if (!grid_barrier(p.gbar, p.spin)) { gave_up = true; break; }
     }
-    // a barrier wait gave up
-    if (threadIdx.x == 0) {
+    if (gave_up && threadIdx.x == 0) {   // a barrier wait gave up
         s->error = 2;
         raise_error(a.err, kErrWaitTimeout);
     }
