@@ -52,7 +52,7 @@ enum hb_status {
 };
 
 enum hb_precision {
-    HB_FP64 = 0,    /* plain FP64 interaction and accumulation (the judge)   */
+    HB_FP64 = 0,    /* plain FP64 interaction and accumulation (the default) */
     HB_MIXED = 1,   /* FP64 predictor; hi/lo FP32 relative positions; FP32
                        interaction; FP32 partial sums flushed into FP64
                        accumulators; FP64 crackle accumulation at 8th order  */
