@@ -647,7 +647,10 @@ persistent_kernel(PersistArgs p)
         if (!grid_barrier(p.gbar, p.spin)) { gave_up = true; break; }
         if (!live) {                     // every CTA reads the same state
             // as the graph engine leaves a step past tend
-            if (blockIdx.x == 0 && threadIdx.x == 0) s->tnext_bits = kInfBits;
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                s->tnext_bits = kInfBits;
+                s->status->error = s->error;   // an error set after the last status write
+            }
             return;
         }
         const int nact = s->nact;
