@@ -142,6 +142,29 @@ __device__ __forceinline__ void load_i_mixed(const float *pred, int ci, int lane
     }
 }
 
+// Compensated (Kahan) accumulation of FP64 partial sums: `tot` carries the
+// running sum of a long j range and `cmp` its lost low-order part, so the
+// sum over all j stays within a few ulp of exact however long the range.
+// (Plain sequential FP64 over 2^20 terms of one sign drifts by ~1e-14
+// relative -- at a particle far outside the cluster, 4e-14 against 3e-16
+// for 84 blocks of 2^20/84 -- and the 8th-order corrector amplifies the
+// step-to-step part of that by up to dt^-7.)  `part` is added and cleared.
+template <int NI, int F>
+__device__ __forceinline__ void kahan_fold(double (&tot)[NI][F], double (&cmp)[NI][F],
+                                           double (&part)[NI][F])
+{
+#pragma unroll
+    for (int n = 0; n < NI; ++n)
+#pragma unroll
+        for (int c = 0; c < F; ++c) {
+            const double y = __dsub_rn(part[n][c], cmp[n][c]);
+            const double t = __dadd_rn(tot[n][c], y);
+            cmp[n][c] = __dsub_rn(__dsub_rn(t, tot[n][c]), y);
+            tot[n][c] = t;
+            part[n][c] = 0.0;
+        }
+}
+
 // One 32-slot j chunk (in shared memory) against this thread's NI i-particles.
 template <int ORDER, int NI>
 __device__ __forceinline__ void chunk64(const double *cp, const Body64 (&I)[NI],

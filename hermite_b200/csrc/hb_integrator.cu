@@ -188,6 +188,15 @@ struct ItemsArgs {
 template <int ORDER, bool MIXED>
 using ItemsShape = ForceShape<ORDER, MIXED, 4, 1, 4, 4, true>;
 
+// FP64 j-sums of the 8th-order schemes are Kahan-compensated per tile
+// (kahan_fold): their corrector turns step-to-step rounding noise of the
+// force into the timestep criterion with factors up to dt^-7 (an outer
+// particle of the 8th-order N = 2^20 configuration reached a timestep
+// below 2^-48 on plain sums over 2^20 terms).  Lower orders keep plain sums
+// and their occupancy.
+template <int ORDER, bool MIXED>
+constexpr bool kKahan = !MIXED && ORDER >= 8;
+
 // The work items of one step with 1..big_nact active slots, taken by this CTA
 // until none are left.  smem: ItemsShape's layout; bar: two initialised
 // mbarriers whose phases continue from g (tiles issued by this CTA before).
@@ -240,9 +249,9 @@ __device__ __forceinline__ bool items_phase(const ItemsArgs &a, unsigned char *s
         else load_i64<ORDER>(reinterpret_cast<const double *>(ptile), 0, lane, I[0]);
         __syncthreads();
 
-        double f[1][F];
+        double f[1][F], tot[1][F], cmp[1][F];   // FP64: per-tile sums, Kahan-folded
 #pragma unroll
-        for (int c = 0; c < F; ++c) f[0][c] = 0.0;
+        for (int c = 0; c < F; ++c) f[0][c] = tot[0][c] = cmp[0][c] = 0.0;
         const int c0 = (int)(((long long)sl * a.nchunk) / S);
         const int c1 = (int)(((long long)(sl + 1) * a.nchunk) / S);
         const int ntile = (c1 - c0 + TCH - 1) / TCH;
@@ -273,6 +282,7 @@ __device__ __forceinline__ bool items_phase(const ItemsArgs &a, unsigned char *s
                 else
                     chunk64<ORDER, 1>(reinterpret_cast<const double *>(ptile + q * CB), I, eps2, f);
             }
+            if constexpr (kKahan<ORDER, MIXED>) kahan_fold<1, F>(tot, cmp, f);
             __syncthreads();
         }
         if (failed_at >= 0) {
@@ -285,6 +295,10 @@ __device__ __forceinline__ bool items_phase(const ItemsArgs &a, unsigned char *s
             return false;
         }
         g += ntile;
+        if constexpr (kKahan<ORDER, MIXED>) {
+#pragma unroll
+            for (int c = 0; c < F; ++c) f[0][c] = __dsub_rn(tot[0][c], cmp[0][c]);
+        }
 
         // the 4 warps' j quarters, in warp order
         double *red = reinterpret_cast<double *>(smem);
@@ -408,11 +422,11 @@ __device__ __forceinline__ bool big_phase(const ItemsArgs &a, unsigned char *sme
         }
         __syncthreads();
 
-        double f[NI][F];
+        double f[NI][F], tot[NI][F], cmp[NI][F];   // FP64: per-tile sums, Kahan-folded
 #pragma unroll
         for (int n = 0; n < NI; ++n)
 #pragma unroll
-            for (int c = 0; c < F; ++c) f[n][c] = 0.0;
+            for (int c = 0; c < F; ++c) f[n][c] = tot[n][c] = cmp[n][c] = 0.0;
         const int c0 = (int)(((long long)sl * a.nchunk) / S);
         const int c1 = (int)(((long long)(sl + 1) * a.nchunk) / S);
         const int ntile = (c1 - c0 + TCH - 1) / TCH;
@@ -443,6 +457,7 @@ __device__ __forceinline__ bool big_phase(const ItemsArgs &a, unsigned char *sme
                 else
                     chunk64<ORDER, NI>(reinterpret_cast<const double *>(ptile + q * CB), I, eps2, f);
             }
+            if constexpr (kKahan<ORDER, MIXED>) kahan_fold<NI, F>(tot, cmp, f);
             __syncthreads();
         }
         if (failed_at >= 0) {
@@ -455,6 +470,12 @@ __device__ __forceinline__ bool big_phase(const ItemsArgs &a, unsigned char *sme
             return false;
         }
         g += ntile;
+        if constexpr (kKahan<ORDER, MIXED>) {
+#pragma unroll
+            for (int n = 0; n < NI; ++n)
+#pragma unroll
+                for (int c = 0; c < F; ++c) f[n][c] = __dsub_rn(tot[n][c], cmp[n][c]);
+        }
 
         if (S == 1) {
 #pragma unroll
@@ -577,8 +598,8 @@ struct PersistSmem {
 // resets the counter and advances the generation (release), which the others
 // poll (acquire).  The CTA barriers on both sides carry the ordering to the
 // CTA's other threads, so every write made before the barrier anywhere in the
-// grid is visible to every read after it (the acquire also drops stale L1
-// lines).  A wait is bounded: after `spin` polls the CTA reports false (the
+// grid is visible to every read after it, the bulk copies that thread 0
+// issues included (proxy fences).  A wait is bounded: after `spin` polls the CTA reports false (the
 // caller raises the error and returns; the other CTAs then give up at their
 // next barrier).
 __device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned *p)
@@ -594,11 +615,20 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p)
     return v;
 }
 
+__device__ __forceinline__ void fence_proxy_async_global()
+{
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
 __device__ __forceinline__ bool grid_barrier(unsigned *gbar, unsigned spin)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
+        // The phases read records with bulk copies (async proxy) that other
+        // CTAs wrote with ordinary stores (generic proxy): proxy fences on
+        // both sides of the barrier order the two.
+        fence_proxy_async_global();
         const unsigned my = ld_relaxed_gpu(gbar + 1);
         unsigned old;
         asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;"
@@ -617,6 +647,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *gbar, unsigned spin)
                 __nanosleep(64);
             }
         }
+        fence_proxy_async_global();
         s_ok = ok;
     }
     __syncthreads();

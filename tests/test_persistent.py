@@ -32,6 +32,14 @@ def _run(order, n, precision, engine, eps, eta, eta_s, dtmax, tend, seed=0, max_
     return stats, rec, dt
 
 
+def test_graph_engine_is_deterministic():
+    """The premise of the comparisons below: two graph-engine runs from the
+    same state agree bit for bit."""
+    a = _run(4, 20000, "fp64", "graph", 4 / 20000, 0.02, 0.005, 1 / 16, 1 / 256)
+    b = _run(4, 20000, "fp64", "graph", 4 / 20000, 0.02, 0.005, 1 / 16, 1 / 256)
+    assert a[0] == b[0] and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+
+
 @pytest.mark.parametrize("order,n,precision,eps,eta,eta_s,dtmax,tend", [
     (4, 1024, "fp64", 1 / 256, 0.01, 0.0025, 1 / 8, 1 / 8),        # c1 to 1/8: > 4096 steps
     (4, 20000, "fp64", 4 / 20000, 0.02, 0.005, 1 / 16, 1 / 256),
