@@ -129,41 +129,51 @@ __global__ void sched_compact_kernel(const double *__restrict__ jp, const double
 }
 
 // Sum of the S slice partials of one i-tile (V values, slice stride sstride
-// doubles) by the T threads of the last CTA to finish it.  With few values
-// the slices are split among thread groups (g, g+G, g+2G, ...) whose sums
-// are added in group order through red[T]; the order is fixed either way.
+// doubles) by the T threads of the last CTA to finish it.  Every value is
+// summed in the same association whatever V is: kGroups interleaved partial
+// sums (slices g, g + kGroups, ...), each in slice order, then added in group
+// order.  (The tile a particle lands in, and so V, depends on the order of
+// the active list, which the compaction does not fix; the association must
+// not.)  With few values the groups of one value go to different threads
+// and meet in red[]; the result is the same bits either way.
+constexpr int kGroups = 8;
+
 template <int T>
 __device__ __forceinline__ void sum_slices(const double *pbase, size_t sstride, int S, int V,
                                            double *out, double *red)
 {
     const int tid = threadIdx.x;
-    if (V >= T / 2) {
-        for (int e = tid; e < V; e += T) {
-            double sum = 0.0;
-            int s = 0;
-            for (; s + 4 <= S; s += 4) {
-                const double p0 = __ldcg(pbase + (size_t)(s + 0) * sstride + e);
-                const double p1 = __ldcg(pbase + (size_t)(s + 1) * sstride + e);
-                const double p2 = __ldcg(pbase + (size_t)(s + 2) * sstride + e);
-                const double p3 = __ldcg(pbase + (size_t)(s + 3) * sstride + e);
-                sum += p0; sum += p1; sum += p2; sum += p3;
-            }
-            for (; s < S; ++s) sum += __ldcg(pbase + (size_t)s * sstride + e);
-            out[e] = sum;
-        }
-    } else {
-        const int G = T / V;
+    if (V * kGroups <= T) {
         const int g = tid / V, e = tid % V;
-        if (g < G) {
+        if (g < kGroups) {
             double sum = 0.0;
-            for (int s = g; s < S; s += G) sum += __ldcg(pbase + (size_t)s * sstride + e);
+            for (int s = g; s < S; s += kGroups) sum += __ldcg(pbase + (size_t)s * sstride + e);
             red[tid] = sum;
         }
         __syncthreads();
         if (tid < V) {
             double sum = red[tid];
-            for (int gg = 1; gg < G; ++gg) sum += red[gg * V + tid];
+#pragma unroll
+            for (int gg = 1; gg < kGroups; ++gg) sum += red[gg * V + tid];
             out[tid] = sum;
+        }
+    } else {
+        for (int e = tid; e < V; e += T) {
+            double acc[kGroups];
+#pragma unroll
+            for (int g = 0; g < kGroups; ++g) acc[g] = 0.0;
+            int s = 0;
+            for (; s + kGroups <= S; s += kGroups) {
+#pragma unroll
+                for (int g = 0; g < kGroups; ++g) acc[g] += __ldcg(pbase + (size_t)(s + g) * sstride + e);
+            }
+#pragma unroll
+            for (int g = 0; g < kGroups; ++g)
+                if (s + g < S) acc[g] += __ldcg(pbase + (size_t)(s + g) * sstride + e);
+            double sum = acc[0];
+#pragma unroll
+            for (int g = 1; g < kGroups; ++g) sum += acc[g];
+            out[e] = sum;
         }
     }
 }

@@ -45,8 +45,8 @@ def test_graph_engine_is_deterministic():
     (4, 20000, "fp64", 4 / 20000, 0.02, 0.005, 1 / 16, 1 / 256),
     (4, 4096, "mixed", 4 / 4096, 0.1, 0.01, 1 / 16, 1 / 8),
     (6, 5000, "fp64", 4 / 5000, 0.1, 0.02, 1 / 16, 1 / 64),
-    (8, 3000, "fp64", 4 / 3000, 0.2, 0.04, 1 / 16, 1 / 64),
-    (8, 2048, "mixed", 4 / 2048, 0.2, 0.04, 1 / 16, 1 / 256),
+    (8, 3000, "fp64", 4 / 3000, 0.75, 0.1, 1 / 16, 1 / 64),      # RUN/inp.8th's eta
+    (8, 2048, "mixed", 4 / 2048, 0.75, 0.1, 1 / 16, 1 / 256),
 ])
 def test_persistent_matches_graph(order, n, precision, eps, eta, eta_s, dtmax, tend):
     a = _run(order, n, precision, "graph", eps, eta, eta_s, dtmax, tend)
