@@ -49,6 +49,18 @@ def test_null_context_is_rejected():
     assert lib.hb_predict_all(None, 0.0) == 1
     assert lib.hb_force_first_nact(None, 1, 0.0, None) == 1
     assert lib.hb_destroy(None) == 0
+    assert lib.hb_set_wait_limit(None, 0) == 1
+    assert lib.hb_integrator_set_engine(None, 3, 0) == 1       # HB_ENGINE_PERSISTENT
+
+
+def test_engine_names_match_the_header():
+    """The Python engine names map to the header's HB_ENGINE_* values."""
+    import re
+    from pathlib import Path
+    header = (Path(hb.__file__).resolve().parent.parent / "include" / "hermite_b200.h").read_text()
+    enum = re.search(r"enum \{ HB_ENGINE_AUTO = 0,[^}]*\}", header).group(0)
+    values = {m.group(1).lower(): int(m.group(2)) for m in re.finditer(r"HB_ENGINE_(\w+) = (\d+)", enum)}
+    assert values == {k: v for k, v in hb.ENGINES.items()}
 
 
 def test_no_device_is_reported(cuda_ok):
