@@ -5,13 +5,8 @@
 // Forces come from the oracle (oracle/hermite_oracle.c: the FP64
 // restatement of the reference's generic Gravity), then, by environment:
 //   HB_NOISE_MODE=fp64      the oracle's FP64 force (default)
-//   HB_NOISE_MODE=fp32pair  the mixed-precision kernel's pair arithmetic
-//                           (hermite_b200/csrc/hb_math.cuh interact_mixed),
-//                           restated in C float: hi/lo FP32 positions, FP32
-//                           velocities [, accelerations [, jerks]], FP32
-//                           interaction, FP32 partial sums over 32 j per
-//                           lane pair flushed into FP64 (the crackle term
-//                           in FP64 per pair), rsqrt correctly rounded
+//   HB_NOISE_MODE=fp32pair  the mixed-precision kernel's pair arithmetic,
+//                           restated in C float (fp32pair.h)
 //   HB_NOISE_MODE=dr32      FP64 pair arithmetic except that the relative
 //                           position is the mixed kernel's hi/lo FP32
 //                           difference (one FP32 rounding per component)
@@ -28,6 +23,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <vector>
+
+#include "fp32pair.h"
 
 extern "C" {
 void oracle_predict(int order, int n, const double *rec, double tsys, double *pred);
@@ -75,73 +72,6 @@ struct Gravity {
     }
 
     void predict_all(double tsys) { oracle_predict(ORDER, nbody, rec.data(), tsys, pred.data()); }
-
-    // The pair arithmetic of the mixed-precision kernel for i-particle i.
-    void force_fp32pair(int i, float eps2, double *f) const
-    {
-        const double *pi = &pred[(size_t)i * NPRED];
-        float nxh[3], nxl[3], nv[3], na[3], nj[3];
-        for (int k = 0; k < 3; ++k) {
-            const float h = (float)pi[k];
-            nxh[k] = -h;
-            nxl[k] = -(float)(pi[k] - (double)h);
-            nv[k] = -(float)pi[4 + k];
-            na[k] = ORDER >= 6 ? -(float)pi[7 + k] : 0.f;
-            nj[k] = ORDER >= 8 ? -(float)pi[10 + k] : 0.f;
-        }
-        for (int c = 0; c < NFORCE; ++c) f[c] = 0.0;
-        const int FS = ORDER == 8 ? 9 : NFORCE;     // FP32-summed words
-        for (int c0 = 0; c0 < nbody; c0 += 32) {
-            float s[2][12] = {};                    // the two halves of a packed pair
-            for (int jl = 0; jl < 32 && c0 + jl < nbody; ++jl) {
-                const double *pj = &pred[(size_t)(c0 + jl) * NPRED];
-                float dr[3], dv[3], da[3] = {0, 0, 0}, dj[3] = {0, 0, 0};
-                for (int k = 0; k < 3; ++k) {
-                    const float h = (float)pj[k], l = (float)(pj[k] - (double)h);
-                    dr[k] = (h + nxh[k]) + (l + nxl[k]);
-                    dv[k] = (float)pj[4 + k] + nv[k];
-                    if (ORDER >= 6) da[k] = (float)pj[7 + k] + na[k];
-                    if (ORDER >= 8) dj[k] = (float)pj[10 + k] + nj[k];
-                }
-                const float m = (float)pj[3];
-                float *a = s[jl & 1];
-                const float r2 = fmaf(dr[2], dr[2], fmaf(dr[1], dr[1], fmaf(dr[0], dr[0], eps2)));
-                const float rv = fmaf(dr[2], dv[2], fmaf(dr[1], dv[1], dr[0] * dv[0]));
-                const float ri = (float)(1.0 / std::sqrt((double)r2));
-                const float ri2 = ri * ri, mr3 = (m * ri) * ri2, al = rv * ri2, al3 = al * -3.0f;
-                float t[3];
-                for (int k = 0; k < 3; ++k) {
-                    a[k] = fmaf(mr3, dr[k], a[k]);
-                    t[k] = fmaf(al3, dr[k], dv[k]);
-                    a[3 + k] = fmaf(mr3, t[k], a[3 + k]);
-                }
-                if (ORDER >= 6) {
-                    const float vv = fmaf(dv[2], dv[2], fmaf(dv[1], dv[1], dv[0] * dv[0]));
-                    const float ra = fmaf(dr[2], da[2], fmaf(dr[1], da[1], dr[0] * da[0]));
-                    const float be = fmaf(al, al, (vv + ra) * ri2);
-                    const float al6 = al3 + al3, be3 = be * -3.0f;
-                    float u[3];
-                    for (int k = 0; k < 3; ++k) {
-                        u[k] = fmaf(be3, dr[k], fmaf(al6, t[k], da[k]));
-                        a[6 + k] = fmaf(mr3, u[k], a[6 + k]);
-                    }
-                    if (ORDER >= 8) {
-                        const float va = fmaf(dv[2], da[2], fmaf(dv[1], da[1], dv[0] * da[0]));
-                        const float rj = fmaf(dr[2], dj[2], fmaf(dr[1], dj[1], dr[0] * dj[0]));
-                        const float g0 = fmaf(3.0f, va, rj) * ri2;
-                        const float g1 = fmaf(al * -4.0f, al, be * 3.0f);
-                        const float ga3 = fmaf(al, g1, g0) * -3.0f;
-                        for (int k = 0; k < 3; ++k) {
-                            const float w = fmaf(ga3, dr[k], fmaf(be * -9.0f, t[k],
-                                                 fmaf(al * -9.0f, u[k], dj[k])));
-                            f[9 + k] += (double)(mr3 * w);
-                        }
-                    }
-                }
-            }
-            for (int c = 0; c < FS; ++c) f[c] += (double)s[0][c] + (double)s[1][c];
-        }
-    }
 
     // FP64 pair arithmetic (the oracle's algebra, SRC/hermite4.h:342-357,
     // SRC/hermite6.h:332-360, SRC/hermite8.h:385-425) on a relative position
@@ -219,7 +149,8 @@ struct Gravity {
         double *out = reinterpret_cast<double *>(force);
         if (fp32pair) {
 #pragma omp parallel for schedule(dynamic, 8)
-            for (int i = 0; i < nact; ++i) force_fp32pair(i, (float)eps2, out + (size_t)i * NFORCE);
+            for (int i = 0; i < nact; ++i)
+                fp32pair_force_one(ORDER, nbody, pred.data(), i, (float)eps2, 0, out + (size_t)i * NFORCE);
         } else if (dr32) {
 #pragma omp parallel for schedule(dynamic, 8)
             for (int i = 0; i < nact; ++i) force_dr32(i, eps2, out + (size_t)i * NFORCE);

@@ -107,3 +107,48 @@ def test_sixth_order(apps, tmp_path):
     assert quiet is not None and quiet[0] <= 1.1 * bs64
     assert run(apps, tmp_path, env={"HB_NOISE_REL": 1e-10}, max_calls=cap, **C3S) is None
     assert run(apps, tmp_path, env={"HB_NOISE_MODE": "fp32pair"}, max_calls=cap, **C3S) is None
+
+
+def _fp32pair_lib():
+    import ctypes
+    r = subprocess.run(["make", "-C", str(NOISE), "lib"], capture_output=True, text=True)
+    if r.returncode != 0:
+        pytest.fail(f"building tests/noise lib failed:\n{r.stderr[-2000:]}")
+    lib = ctypes.CDLL(str(NOISE / "_build" / "libfp32pair.so"))
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.fp32pair_force.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ctypes.c_double,
+                                   ctypes.c_int, dp]
+    lib.fp32pair_force.restype = None
+    return lib
+
+
+def test_split_velocities_do_not_change_fp32_errors(oracle):
+    """Hi/lo velocities and accelerations (formed like the hi/lo positions)
+    leave the FP32 pair arithmetic's per-evaluation errors where they are:
+    the rounding of the pair terms themselves dominates.  6th order, Plummer
+    N = 4096 with acc/jrk/snp from the oracle's forces (the integrator's
+    start-up), eps = 1/4096."""
+    import ctypes
+    import numpy as np
+    from hermite_b200.ic import plummer, records
+    lib = _fp32pair_lib()
+    order, n, eps2 = 6, 4096, (1 / 4096) ** 2
+    rec = records(plummer(n, 2), order)
+    for _ in range(2):                      # acc, jrk; then snp with acc in the records
+        f = oracle.predict_force(order, rec, 0.0, n, eps2)
+        rec[:, 8:17] = f[:, 0:9]
+    pred = np.ascontiguousarray(oracle.predict(order, rec, 0.0))
+    ref = oracle.force(order, pred, n, eps2)
+    dp = ctypes.POINTER(ctypes.c_double)
+    err = {}
+    for split in (0, 1):
+        got = np.empty_like(ref)
+        lib.fp32pair_force(order, n, pred.ctypes.data_as(dp), n, eps2, split,
+                           got.ctypes.data_as(dp))
+        e = np.linalg.norm((got - ref).reshape(n, 3, 3), axis=2) / \
+            np.linalg.norm(ref.reshape(n, 3, 3), axis=2)
+        err[split] = (np.median(e, axis=0), e.max(axis=0))
+    for k in range(3):                      # acc, jrk, snp
+        med0, med1 = err[0][0][k], err[1][0][k]
+        assert abs(med1 - med0) <= 0.15 * med0, (k, med0, med1)
+        assert err[1][1][k] >= 0.5 * err[0][1][k], (k, err[0][1][k], err[1][1][k])
