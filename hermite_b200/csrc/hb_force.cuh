@@ -165,6 +165,14 @@ __device__ __forceinline__ void kahan_fold(double (&tot)[NI][F], double (&cmp)[N
         }
 }
 
+// The FP64 j-sums of the 8th-order schemes are Kahan-compensated per tile:
+// their corrector turns step-to-step rounding noise of the force into the
+// timestep criterion with factors up to dt^-7 (an outer particle of the
+// 8th-order N = 2^20 configuration reached a timestep below 2^-48 on plain
+// sums over 2^20 terms).  Lower orders keep plain sums and their occupancy.
+template <int ORDER, bool MIXED>
+constexpr bool kKahan = !MIXED && ORDER >= 8;
+
 // One 32-slot j chunk (in shared memory) against this thread's NI i-particles.
 template <int ORDER, int NI>
 __device__ __forceinline__ void chunk64(const double *cp, const Body64 (&I)[NI],
@@ -364,12 +372,14 @@ force_kernel(ForceArgs a)
     const int ntile = (c1 - c0 + TCH - 1) / TCH;
     const int ichunk0 = (blockIdx.x * TI) / 32 + ig * NI;   // first i chunk of this warp
 
-    // i-particles and accumulators
-    double f[NI][F];
+    // i-particles and accumulators (8th order FP64: per-tile sums in f,
+    // Kahan-folded into tot/cmp)
+    constexpr bool KAHAN = kKahan<ORDER, MIXED>;
+    double f[NI][F], tot[NI][F], cmp[NI][F];
 #pragma unroll
     for (int n = 0; n < NI; ++n)
 #pragma unroll
-        for (int c = 0; c < F; ++c) f[n][c] = 0.0;
+        for (int c = 0; c < F; ++c) f[n][c] = tot[n][c] = cmp[n][c] = 0.0;
 
     using IBody = typename std::conditional<MIXED, NegI32, Body64>::type;
     IBody I[NI];
@@ -453,6 +463,7 @@ force_kernel(ForceArgs a)
             else
                 chunk64<ORDER, NI>(reinterpret_cast<const double *>(tile + q * CB), I, a.eps2, f);
         }
+        if constexpr (KAHAN) kahan_fold<NI, F>(tot, cmp, f);
         __syncthreads();
         if (!FUSED && tid == 0 && t + STG < ntile) issue(t + STG);
     }
@@ -464,6 +475,12 @@ force_kernel(ForceArgs a)
                 mbar_wait_bounded(&bar[t % STG], (uint32_t)((t / STG) & 1));
         }
         return;
+    }
+    if constexpr (KAHAN) {
+#pragma unroll
+        for (int n = 0; n < NI; ++n)
+#pragma unroll
+            for (int c = 0; c < F; ++c) f[n][c] = __dsub_rn(tot[n][c], cmp[n][c]);
     }
 
     force_epilogue<ORDER, NW, NI, WJ, WI, TI>(f, smem, a, ig, jg, ichunk0);

@@ -198,14 +198,7 @@ struct ItemsArgs {
 template <int ORDER, bool MIXED>
 using ItemsShape = ForceShape<ORDER, MIXED, 4, 1, 4, 4, true>;
 
-// FP64 j-sums of the 8th-order schemes are Kahan-compensated per tile
-// (kahan_fold): their corrector turns step-to-step rounding noise of the
-// force into the timestep criterion with factors up to dt^-7 (an outer
-// particle of the 8th-order N = 2^20 configuration reached a timestep
-// below 2^-48 on plain sums over 2^20 terms).  Lower orders keep plain sums
-// and their occupancy.
-template <int ORDER, bool MIXED>
-constexpr bool kKahan = !MIXED && ORDER >= 8;
+// (8th-order FP64 j-sums are Kahan-compensated per tile: kKahan, hb_force.cuh)
 
 // The work items of one step with 1..big_nact active slots, taken by this CTA
 // until none are left.  smem: ItemsShape's layout; bar: two initialised
