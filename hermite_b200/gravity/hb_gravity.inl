@@ -94,8 +94,10 @@ struct Gravity {
     // the GPU; the integrator's barrier after the prediction, and the barrier
     // here after the force, keep the others in step.  Above
     // NACT_PARALLEL_THRESH active particles the integrator spreads set_jp over
-    // the threads, which set_jp allows for distinct slots.
-    enum { NACT_PARALLEL_THRESH = 8 };
+    // the threads, which set_jp allows for distinct slots; the thresholds are
+    // the reference's AVX backends' (8 at 4th order, 12 at 6th and 8th:
+    // SRC/hermite4-avx.h:9, SRC/hermite6-avx.h:9, SRC/hermite8-avx.h:10).
+    enum { NACT_PARALLEL_THRESH = HB_GRAVITY_ORDER == 4 ? 8 : 12 };
 
     void predict_all_fast_omp(const double tsys)
     {
