@@ -338,9 +338,9 @@ ens_force_kernel(EnsLaunch L)
         else load_i64<ORDER>(reinterpret_cast<const double *>(ptile), 0, lane, I[0]);
         __syncthreads();
 
-        double f[1][F];
+        double f[1][F], tot[1][F], cmp[1][F];   // 8th order FP64: Kahan-folded per tile
 #pragma unroll
-        for (int q = 0; q < F; ++q) f[0][q] = 0.0;
+        for (int q = 0; q < F; ++q) f[0][q] = tot[0][q] = cmp[0][q] = 0.0;
         const int cb = cl.off / 32, nch = cl.npad / 32;
         const int c0 = cb + (int)(((long long)sl * nch) / S);
         const int c1 = cb + (int)(((long long)(sl + 1) * nch) / S);
@@ -374,6 +374,7 @@ ens_force_kernel(EnsLaunch L)
                 else
                     chunk64<ORDER, 1>(reinterpret_cast<const double *>(ptile + q * CB), I, eps2, f);
             }
+            if constexpr (kKahan<ORDER, MIXED>) kahan_fold<1, F>(tot, cmp, f);
             __syncthreads();
         }
         if (failed_at >= 0) {
@@ -386,6 +387,10 @@ ens_force_kernel(EnsLaunch L)
             return;
         }
         g += ntile;
+        if constexpr (kKahan<ORDER, MIXED>) {
+#pragma unroll
+            for (int q = 0; q < F; ++q) f[0][q] = __dsub_rn(tot[0][q], cmp[0][q]);
+        }
 
         double *red = reinterpret_cast<double *>(smem);
         if (jg > 0)
