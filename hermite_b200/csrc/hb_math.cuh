@@ -128,9 +128,11 @@ __device__ __forceinline__ void interact64(const Body64 &I, const Body64 &J,
         double da[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) da[k] = J.a[k] - I.a[k];
-        const double vv = fma(dv[2], dv[2], fma(dv[1], dv[1], dv[0] * dv[0]));
-        const double ra = fma(dr[2], da[2], fma(dr[1], da[1], dr[0] * da[0]));
-        const double be = fma(al, al, (vv + ra) * ri2);  // beta
+        // v.v + r.a as one chain of fused multiply-adds (one add fewer than
+        // two dot products and their sum)
+        const double vvra = fma(dr[2], da[2], fma(dr[1], da[1], fma(dr[0], da[0],
+                            fma(dv[2], dv[2], fma(dv[1], dv[1], dv[0] * dv[0])))));
+        const double be = fma(al, al, vvra * ri2);       // beta
         double u[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -216,9 +218,9 @@ __device__ __forceinline__ void interact_mixed(const NegI32 &I, const JPair32 &J
         float2 da[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) da[k] = add2(J.a[k], I.a[k]);
-        const float2 vv = fma2(dv[2], dv[2], fma2(dv[1], dv[1], mul2(dv[0], dv[0])));
-        const float2 ra = fma2(dr[2], da[2], fma2(dr[1], da[1], mul2(dr[0], da[0])));
-        const float2 be = fma2(al, al, mul2(add2(vv, ra), ri2));
+        const float2 vvra = fma2(dr[2], da[2], fma2(dr[1], da[1], fma2(dr[0], da[0],
+                            fma2(dv[2], dv[2], fma2(dv[1], dv[1], mul2(dv[0], dv[0]))))));
+        const float2 be = fma2(al, al, mul2(vvra, ri2));
         const float2 al6 = add2(al3, al3);
         const float2 be3 = mul2(be, f2(-3.0f));
         float2 u[3];

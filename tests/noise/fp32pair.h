@@ -65,9 +65,9 @@ static inline void fp32pair_force_one(int order, int n, const double *pred, int 
                 a[3 + k] = fmaf(mr3, t[k], a[3 + k]);
             }
             if (order >= 6) {
-                const float vv = fmaf(dv[2], dv[2], fmaf(dv[1], dv[1], dv[0] * dv[0]));
-                const float ra = fmaf(dr[2], da[2], fmaf(dr[1], da[1], dr[0] * da[0]));
-                const float be = fmaf(al, al, (vv + ra) * ri2);
+                const float vvra = fmaf(dr[2], da[2], fmaf(dr[1], da[1], fmaf(dr[0], da[0],
+                                   fmaf(dv[2], dv[2], fmaf(dv[1], dv[1], dv[0] * dv[0])))));
+                const float be = fmaf(al, al, vvra * ri2);
                 const float al6 = al3 + al3, be3 = be * -3.0f;
                 for (int k = 0; k < 3; ++k) {
                     u[k] = fmaf(be3, dr[k], fmaf(al6, t[k], da[k]));
