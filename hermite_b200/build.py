@@ -30,7 +30,7 @@ INCLUDE = ROOT / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fopenmp",
               "--expt-relaxed-constexpr", "-I", str(INCLUDE), "-I", str(CSRC)]
-SOURCES = ["hb_capi.cu", "hb_predict_pot.cu", "hb_force_64.cu", "hb_force_mixed.cu",
+SOURCES = ["hb_capi.cu", "hb_predict_pot.cu", "hb_force_64.cu", "hb_force_mixed.cu", "hb_force_lanes.cu",
            "hb_noalloc.cu", "hb_integrator.cu", "hb_ensemble.cu", "hb_team.cu",
            "hb_dump.cu"]
 HEADERS = ["hb_common.cuh", "hb_math.cuh", "hb_force.cuh", "hb_force_table.cuh",

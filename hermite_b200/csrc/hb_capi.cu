@@ -258,6 +258,24 @@ int run_force(hb_ctx *ctx, int nact, double eps2, double *force_out_dev)
 {
     if (nact == 0) return HB_OK;
     const bool mixed = ctx->pred_precision == HB_MIXED;
+    if (!mixed && ctx->order != 9 && nact <= kLanesMaxAct && ctx->variant_override < 0) {
+        // a handful of active particles: lanes share an i-particle
+        ForceArgs a{};
+        a.jp = ctx->d_jp;
+        a.tsys = ctx->tsys;
+        a.nbody = ctx->nbody;
+        a.nchunk = ctx->npad / 32;
+        a.nact = nact;
+        a.eps2 = eps2;
+        a.force = force_out_dev;
+        a.partial = ctx->d_partial;
+        a.counter = ctx->d_counter;
+        a.err = ctx->d_err;
+        a.spin = ctx->wait_limit;
+        HB_CK(launch_force_lanes(ctx->order, a, ctx->nsm, ctx->stream));
+        ctx->launches++;
+        return HB_OK;
+    }
     int jsplit_hint = 0;
     const int v = pick_variant(ctx, nact, &jsplit_hint);
     const ForceVariant *fv = force_variant(ctx->order, mixed, v);

@@ -140,6 +140,13 @@ cudaError_t integrator_energy(int order, const double *jp, const double *pot, in
 int force_variant_count(int order, bool mixed);
 const ForceVariant *force_variant(int order, bool mixed, int v);
 
+// FP64 force for block steps of at most kLanesMaxAct active particles
+// (orders 4, 6, 8): lanes of a warp share an i-particle and split j
+// (hb_force_lanes.cu).  Uses a.jp / a.tsys / a.nbody (it predicts the raw
+// records itself), a.partial for S * kLanesMaxAct * F doubles and a.counter[0].
+constexpr int kLanesMaxAct = 16;
+cudaError_t launch_force_lanes(int order, const ForceArgs &a, int nsm, cudaStream_t s);
+
 cudaError_t launch_predict(int order, bool mixed, const double *jp, int n, int npad,
                            double tsys, void *pred, int *err, cudaStream_t s);
 cudaError_t launch_potential(int order, const double *jp, int n, int npad, double eps2,

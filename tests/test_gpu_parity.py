@@ -83,11 +83,40 @@ def test_potential(order, oracle):
     np.testing.assert_allclose(got, ref, rtol=1e-13, atol=0)
 
 
-@pytest.mark.parametrize("variant", [0, 2, 12, 13])   # two-pass and fused shapes
+@pytest.mark.parametrize("order", [4, 6, 8])
+@pytest.mark.parametrize("n", [1, 5, 33, 1000, 4097, 70000])
+def test_fp64_small_blocks(order, n, oracle):
+    """Block steps of at most 16 active particles take the lane-split kernel
+    (lanes of a warp share an i-particle and split j): every nact up to 16
+    and a few j-slice counts (set by N) against the oracle."""
+    for nact in sorted({1, 2, 3, 5, 8, 13, 16} & set(range(1, n + 1))):
+        _check(order, n, nact, "fp64", oracle, seed=31)
+
+
+@pytest.mark.parametrize("order", [4, 6, 8])
+def test_small_blocks_match_tiled_kernel(order):
+    """The lane-split kernel and the tiled kernel (an explicit shape) agree
+    to summation-order rounding, and the lane-split result is reproducible
+    to the bit."""
+    n = 20000
+    rec = make_records(order, n, seed=41)
+    for nact in (1, 4, 11, 16):
+        out = []
+        for variant in (-1, -1, 0):
+            with Gravity(order, n) as g:
+                g.set_force_shape(variant, 0)
+                g.set_jp_records(rec)
+                g.predict_all(0.0)
+                out.append(g.calc_force_on_first_nact(nact, EPS2))
+        assert np.array_equal(out[0], out[1]), nact
+        assert rel_err(out[0], out[2]).max() <= FP64_TOL, nact
+
+
+@pytest.mark.parametrize("variant", [0, 2, 12, 13, -1])   # two-pass, fused, automatic shapes
 def test_self_term_is_zero(variant):
     """One particle: the force on it is exactly zero in both precisions (the
-    fused kernel predicts i and j separately; the two states must agree to
-    the bit)."""
+    fused kernels predict i and j separately; the two states must agree to
+    the bit).  The automatic shape is the lane-split kernel in FP64."""
     for order in (4, 6, 8):
         rec = make_records(order, 1, seed=2)
         for prec in ("fp64", "mixed"):
