@@ -7,13 +7,15 @@
 // take 6.5 us to stream from HBM).
 //
 // Here a warp's 32 lanes form P groups of G = 32/P lanes, P = nact rounded
-// up to a power of two (nact <= 16, so G >= 2).  The G lanes of group p share
+// up to a power of two (nact <= 16, so G >= 2; from 17 on, one lane per i,
+// the tiled kernel measured faster at N >= 2^18).  The G lanes of group p share
 // i-particle p and take every G-th j of each 32-slot chunk; their partial
 // sums meet in a fixed xor-shuffle tree.  Each warp predicts its own chunks
 // from the raw records (one lane per slot) into shared memory, so a launch
-// reads every j record once.  The CTAs of the grid are j-slices; the last
-// one to finish adds the slices' partials in slice order.  Every sum has a
-// fixed association for a given (nact, N), so results are deterministic.
+// reads every j record once, and the warps of a CTA take the chunks of its
+// j-slice in turn.  The CTAs of the grid are j-slices; the last one to finish
+// adds the slices' partials, spread over its threads.  Every sum has a fixed
+// association for a given (nact, N), so results are deterministic.
 //
 // The same job as the reference's force_kernel with its j-blocks
 // (SRC/hermite4-titan.cu:189-238, SRC/hermite6-titan.cu:245-299,
@@ -26,7 +28,7 @@
 namespace hb {
 namespace {
 
-constexpr int kLanesWarps = 4;
+constexpr int kLanesWarps = 8;
 
 // Predicts the 32 slots of chunk `chunk` (one per lane) into the predicted
 // FP64 chunk layout at dst.  Out of line: the i-particles come from the same
@@ -59,18 +61,23 @@ __device__ __noinline__ void predict_chunk_warp(const double *jp, int chunk, int
     c[P64_M * 32] = m;
 }
 
-template <int ORDER>
+template <int ORDER, int LOG2G>
 __global__ void __launch_bounds__(kLanesWarps * 32)
-force_lanes_kernel(ForceArgs a, int log2g)
+force_lanes_kernel(ForceArgs a)
 {
+    constexpr int G = 1 << LOG2G, P = 32 / G;
     constexpr int F = Frc<ORDER>::words, NC = Pred64<ORDER>::ncomp;
-    __shared__ double chunk[kLanesWarps][NC * 32];
-    __shared__ double red[kLanesWarps][kLanesMaxAct][F];
+    // per warp: one predicted chunk; after the j loop the same space holds
+    // the warps' group sums, then the cross-slice group sums
+    constexpr int kWords = kLanesWarps * NC * 32;
+    static_assert(kWords >= kLanesWarps * kLanesMaxAct * F, "reduction space");
+    static_assert(kWords >= 2 * kLanesWarps * 32 && kWords >= kLanesMaxAct * F, "slice sums");
+    __shared__ double sm[kWords];
     __shared__ unsigned s_last;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int G = 1 << log2g, p = lane >> log2g, g = lane & (G - 1);
+    const int p = lane >> LOG2G, g = lane & (G - 1);
     const int S = gridDim.x, sl = blockIdx.x, nact = a.nact;
-    double *my = chunk[w];
+    double *my = sm + w * NC * 32;
 
     // i-particle p (lanes of groups p >= nact compute a copy of the last one
     // and are dropped at the end); the i-particles are slots 0..nact-1 of chunk 0
@@ -88,28 +95,31 @@ force_lanes_kernel(ForceArgs a, int log2g)
     for (int c = c0 + w; c < c1; c += kLanesWarps) {
         predict_chunk_warp<ORDER>(a.jp, c, a.nbody, a.tsys, my);
         __syncwarp();
-        for (int k = g; k < 32; k += G) {
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
             Body64 J;
-            load_i64<ORDER>(my, 0, k, J);
+            load_i64<ORDER>(my, 0, g + k * G, J);
             interact64<ORDER>(I, J, a.eps2, f);
         }
         __syncwarp();
     }
     // the G lanes of a group: a fixed butterfly
+#pragma unroll
     for (int o = G >> 1; o > 0; o >>= 1)
 #pragma unroll
         for (int q = 0; q < F; ++q) f[q] += __shfl_xor_sync(0xffffffffu, f[q], o);
+    __syncthreads();                     // every warp is done with its chunk
+    double *red = sm;                    // [warp][i][F]
     if (g == 0 && p < nact)
 #pragma unroll
-        for (int q = 0; q < F; ++q) red[w][p][q] = f[q];
+        for (int q = 0; q < F; ++q) red[(w * kLanesMaxAct + p) * F + q] = f[q];
     __syncthreads();
 
     const int V = nact * F;
     for (int e = tid; e < V; e += blockDim.x) {
-        const int pp = e / F, q = e - pp * F;
-        double v = red[0][pp][q];
+        double v = red[e];
 #pragma unroll
-        for (int ww = 1; ww < kLanesWarps; ++ww) v += red[ww][pp][q];
+        for (int ww = 1; ww < kLanesWarps; ++ww) v += red[ww * kLanesMaxAct * F + e];
         if (S == 1) a.force[e] = v;
         else a.partial[(size_t)sl * kLanesMaxAct * F + e] = v;
     }
@@ -120,9 +130,28 @@ force_lanes_kernel(ForceArgs a, int log2g)
     __syncthreads();
     if (!s_last) return;
     __threadfence();
+    // the slices' sum, spread over the CTA: thread t = k*V + e adds slices
+    // k, k+K, ... of value e into 8 interleaved sums (8 loads in flight),
+    // combined pairwise; then each value's K group sums in group order
+    const int K = max(1, (int)blockDim.x / V);
+    double *grp = sm;
+    for (int t = tid; t < K * V; t += blockDim.x) {
+        const int k = t / V, e = t - k * V;
+        double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int s2 = k;
+        for (; s2 + 7 * K < S; s2 += 8 * K)
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                acc[u] += __ldcg(a.partial + (size_t)(s2 + u * K) * kLanesMaxAct * F + e);
+#pragma unroll
+        for (int u = 0; u < 7; ++u)
+            if (s2 + u * K < S) acc[u] += __ldcg(a.partial + (size_t)(s2 + u * K) * kLanesMaxAct * F + e);
+        grp[t] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    }
+    __syncthreads();
     for (int e = tid; e < V; e += blockDim.x) {
-        double v = 0.0;
-        for (int s2 = 0; s2 < S; ++s2) v += __ldcg(a.partial + (size_t)s2 * kLanesMaxAct * F + e);
+        double v = grp[e];
+        for (int k = 1; k < K; ++k) v += grp[k * V + e];
         a.force[e] = v;
     }
     if (tid == 0) a.counter[0] = 0u;
@@ -135,15 +164,20 @@ cudaError_t launch_force_lanes(int order, const ForceArgs &a, int nsm, cudaStrea
     if (a.nact < 1 || a.nact > kLanesMaxAct || a.nchunk < 1) return cudaErrorInvalidValue;
     int log2g = 5;
     while ((1 << (5 - log2g)) < a.nact) --log2g;          // P = 2^(5 - log2g) >= nact
-    // one CTA per two chunks a warp, at most two CTAs per SM
+    // j-slices of at least two chunks a warp, at most two CTAs per SM
     const int S = std::max(1, std::min(2 * nsm, a.nchunk / (2 * kLanesWarps)));
     const dim3 grid(S), block(kLanesWarps * 32);
-    switch (order) {
-    case 4: force_lanes_kernel<4><<<grid, block, 0, s>>>(a, log2g); break;
-    case 6: force_lanes_kernel<6><<<grid, block, 0, s>>>(a, log2g); break;
-    case 8: force_lanes_kernel<8><<<grid, block, 0, s>>>(a, log2g); break;
-    default: return cudaErrorInvalidValue;
-    }
+    using K = void (*)(ForceArgs);
+    static const K table[3][6] = {
+        {force_lanes_kernel<4, 0>, force_lanes_kernel<4, 1>, force_lanes_kernel<4, 2>,
+         force_lanes_kernel<4, 3>, force_lanes_kernel<4, 4>, force_lanes_kernel<4, 5>},
+        {force_lanes_kernel<6, 0>, force_lanes_kernel<6, 1>, force_lanes_kernel<6, 2>,
+         force_lanes_kernel<6, 3>, force_lanes_kernel<6, 4>, force_lanes_kernel<6, 5>},
+        {force_lanes_kernel<8, 0>, force_lanes_kernel<8, 1>, force_lanes_kernel<8, 2>,
+         force_lanes_kernel<8, 3>, force_lanes_kernel<8, 4>, force_lanes_kernel<8, 5>}};
+    const int oi = order == 4 ? 0 : order == 6 ? 1 : order == 8 ? 2 : -1;
+    if (oi < 0) return cudaErrorInvalidValue;
+    table[oi][log2g]<<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
 

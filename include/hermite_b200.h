@@ -158,7 +158,11 @@ int hb_set_wait_limit(hb_ctx *ctx, long long polls);
 /* Launch shape of the force kernel, picked per (order, precision, nbody,
  * nact) by the built-in tuning table unless overridden here.  variant
  * indexes the compiled kernel variants (see hb_force_variant_count);
- * jsplit is the number of j-slices (CTAs per i-tile); 0 means "auto". */
+ * jsplit is the number of j-slices (CTAs per i-tile); 0 means "auto".
+ * With variant < 0 (automatic), FP64 block steps of at most 16 active
+ * particles (orders 4, 6, 8) take a separate kernel in which the lanes of
+ * a warp share an i-particle and split the j range; an explicit variant
+ * always takes the tiled kernel. */
 int hb_set_force_shape(hb_ctx *ctx, int variant, int jsplit);
 int hb_force_variant_count(int order, int precision);
 /* Describe a variant: threads per CTA, i per thread, warps splitting j. */

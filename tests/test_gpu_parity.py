@@ -87,9 +87,10 @@ def test_potential(order, oracle):
 @pytest.mark.parametrize("n", [1, 5, 33, 1000, 4097, 70000])
 def test_fp64_small_blocks(order, n, oracle):
     """Block steps of at most 16 active particles take the lane-split kernel
-    (lanes of a warp share an i-particle and split j): every nact up to 16
-    and a few j-slice counts (set by N) against the oracle."""
-    for nact in sorted({1, 2, 3, 5, 8, 13, 16} & set(range(1, n + 1))):
+    (lanes of a warp share an i-particle and split j): nact across every
+    lane-group size and a few j-slice counts (set by N) against the oracle,
+    and the first nact past it (the tiled kernel)."""
+    for nact in sorted({1, 2, 3, 5, 8, 13, 16, 17} & set(range(1, n + 1))):
         _check(order, n, nact, "fp64", oracle, seed=31)
 
 
@@ -100,7 +101,7 @@ def test_small_blocks_match_tiled_kernel(order):
     to the bit."""
     n = 20000
     rec = make_records(order, n, seed=41)
-    for nact in (1, 4, 11, 16):
+    for nact in (1, 2, 4, 11, 16):
         out = []
         for variant in (-1, -1, 0):
             with Gravity(order, n) as g:
