@@ -261,6 +261,32 @@ def traffic_from_profiles(name):
     return None
 
 
+def tiled_shape(order, n, nact):
+    """The tiled force kernel's shape (variant, j-slices) that the library
+    takes from its tuning table for (order, FP64, n, nact): the nearest N
+    bucket, then the nearest nact bucket, the slice count rescaled to the
+    bucket's CTA count (hb_capi.cu, pick_variant)."""
+    import ctypes
+    import math
+    from hermite_b200 import load_library
+    best = None
+    for line in (ROOT / "hermite_b200" / "csrc" / "hb_tuning.inc").read_text().splitlines():
+        if not line.startswith("{"):
+            continue
+        o, m, ln, la, v, sp = (int(x) for x in line.strip("{},").split(","))
+        if o != order or m != 0:
+            continue
+        key = (abs(ln - math.log2(n)), abs(la - math.log2(nact)))
+        if best is None or key < best[0]:
+            best = (key, la, v, sp)
+    _, la, v, sp = best
+    th, ni, wj = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    load_library().hb_force_variant_info(order, 0, v, ctypes.byref(th), ctypes.byref(ni), ctypes.byref(wj))
+    ti = th.value // (32 * wj.value) * 32 * ni.value
+    gx_bucket, gx = -(-(1 << la) // ti), -(-nact // ti)
+    return v, max(1, -(-(gx_bucket * sp) // gx))
+
+
 def timed_steps(g, stream, flush, steps, eps2, t0=0.0):
     """CUDA-event times (ms) of `steps` device-resident steps: L2 flush,
     predict_all to a new time, force on all N."""
@@ -333,19 +359,29 @@ def run_ours(args):
         e2e = nint * args.steps * world / e2e_s * 1e-9
 
         # ---- block-step latency through the C ABI (set_jp + predict_all + force) ----
-        block_us = {}
-        for nact in (1, 32, 1024, 8192, 65536):
+        def block_step_us(nact, reps):
             buf = np.empty((nact, F))
             for _ in range(3):
                 g.predict_all(0.0)
                 g.calc_force_on_first_nact(nact, eps2, buf)
-            reps = 50 if nact <= 8192 else 5
-            t0 = time.perf_counter()
+            times = []
             for _ in range(reps):
+                t0 = time.perf_counter()
                 g.set_jp_records(rec[:nact])
                 g.predict_all(0.0)
                 g.calc_force_on_first_nact(nact, eps2, buf)
-            block_us[str(nact)] = (time.perf_counter() - t0) / reps * 1e6
+                times.append(time.perf_counter() - t0)
+            return statistics.median(times) * 1e6
+        block_us = {str(nact): block_step_us(nact, 200 if nact <= 8192 else 5)
+                    for nact in (1, 4, 16, 32, 1024, 8192, 65536)}
+        # the same small steps on the tiled kernel (the tuning table's shape),
+        # against the lane-split kernel the automatic choice takes
+        block_us_tiled = {}
+        for nact in (1, 4, 16):
+            v, S = tiled_shape(ORDER, N, nact)
+            g.set_force_shape(v, S)
+            block_us_tiled[str(nact)] = block_step_us(nact, 200)
+        g.set_force_shape(-1, 0)
         g.close()
 
         # ---- the same step with the mixed-precision kernel ----
@@ -433,8 +469,9 @@ def run_ours(args):
         "fp32_peak_tflops": fp32_peak * 1e-3,
         "mixed": mixed,
         "block_step_us": {"order": ORDER, "nbody": N, "precision": "fp64",
-                          "through": "set_jp(nact) + predict_all + calc_force_on_first_nact",
-                          "us": block_us},
+                          "through": "set_jp(nact) + predict_all + calc_force_on_first_nact "
+                                     "(Python ctypes calls; median of 200)",
+                          "us": block_us, "us_tiled_kernel": block_us_tiled},
         "config_c4": c4,
         "mixed_force_noise": noise,
         "device_integrator": integ,
