@@ -1,14 +1,17 @@
 """Force parity against the FP64 oracle at the benchmark sizes, on realistic
 states.
 
-c3: 6th order, N = 262144, eps = 1/4096;  c4: 8th order, N = 2^20,
-eps = 1/16384.  The states come from the FP64 device integrator after its
-start-up and a short run (tests/states.py), so acc, jrk, snp [, crk] and the
-spread of tlast are those of a real run.  A random sample of 4096 i-particles
-is moved to the front; both precisions compute their forces against all N
-j-particles, predicted to the integrator's time, and the C oracle
+c1: 4th order, N = 1024, eps = 1/256;  c2: 4th order, N = 65536,
+eps = 1/1024;  c3: 6th order, N = 262144, eps = 1/4096;  c4: 8th order,
+N = 2^20, eps = 1/16384.  The states come from the FP64 device integrator
+after its start-up and a short run (tests/states.py), so acc, jrk, snp
+[, crk] and the spread of tlast are those of a real run.  At c1 and c2 every
+particle is checked; at c3 and c4 a random sample of 4096 i-particles is
+moved to the front.  Both precisions compute the forces on these against all
+N j-particles, predicted to the integrator's time, and the C oracle
 (oracle/hermite_oracle.c, a restatement of the reference's generic Gravity,
-SRC/hermite6.h:332-360, SRC/hermite8.h:385-425) does the same on the CPU.
+SRC/hermite4.h:342-357, SRC/hermite6.h:332-360, SRC/hermite8.h:385-425) does
+the same on the CPU.
 
 Bounds, per derivative, on the maximum and the median over the sample of
 |f - f_oracle| / |f_oracle|:
@@ -30,13 +33,15 @@ import hermite_b200 as hb
 from inputs import rel_err
 from states import CONFIGS, integrator_state, sample_first
 
-NSAMPLE = 4096
+NSAMPLE = {"c1": 1024, "c2": 65536, "c3": 4096, "c4": 4096}   # c1, c2: every particle
 # acc, jrk, snp [, crk]
 FP64_TOL = (1e-12, 1e-12, 1e-12, 1e-9)
 FP64_MEDIAN = 1e-13
-MIXED_TOL = {"c3": (1e-6, 2e-5, 2e-4), "c4": (1e-6, 1.2e-5, 4e-5, 1.5e-2)}
-MIXED_MEDIAN = {"c3": (6e-8, 5e-7, 1e-6), "c4": (6e-8, 5e-7, 1e-6, 1.2e-6)}
-T_RUN = {"c3": 1.0 / 1024, "c4": 1.0 / 4096}
+MIXED_TOL = {"c1": (1e-6, 1e-5), "c2": (1e-6, 1e-5),
+             "c3": (1e-6, 2e-5, 2e-4), "c4": (1e-6, 1.2e-5, 4e-5, 1.5e-2)}
+MIXED_MEDIAN = {"c1": (1e-7, 5e-7), "c2": (1e-7, 5e-7),
+                "c3": (6e-8, 5e-7, 1e-6), "c4": (6e-8, 5e-7, 1e-6, 1.2e-6)}
+T_RUN = {"c1": 1.0 / 64, "c2": 1.0 / 1024, "c3": 1.0 / 1024, "c4": 1.0 / 4096}
 
 _cache = {}
 
@@ -44,22 +49,23 @@ _cache = {}
 def sampled_case(name, oracle):
     if name not in _cache:
         rec, t, eps2 = integrator_state(name, T_RUN[name])
-        recp, _ = sample_first(rec, NSAMPLE, seed=1)
+        ns = NSAMPLE[name]
+        recp = rec if ns == rec.shape[0] else sample_first(rec, ns, seed=1)[0]
         order = CONFIGS[name][0]
-        ref = oracle.predict_force(order, recp, t, NSAMPLE, eps2)
+        ref = oracle.predict_force(order, recp, t, ns, eps2)
         _cache[name] = (order, recp, t, eps2, ref)
     return _cache[name]
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("name", ["c3", "c4"])
+@pytest.mark.parametrize("name", ["c1", "c2", "c3", "c4"])
 def test_sample_against_oracle(name, precision, oracle):
     order, recp, t, eps2, ref = sampled_case(name, oracle)
     with hb.Gravity(order, recp.shape[0], precision) as g:
         g.set_jp_records(recp)
         g.predict_all(t)
-        got = g.calc_force_on_first_nact(NSAMPLE, eps2)
+        got = g.calc_force_on_first_nact(NSAMPLE[name], eps2)
     assert np.all(np.isfinite(got))
     err = rel_err(got, ref)
     print(f"{name} {precision}: max", " ".join(f"{e:.2e}" for e in err.max(axis=0)),
