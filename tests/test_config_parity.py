@@ -20,11 +20,15 @@ Bounds, per derivative, on the maximum and the median over the sample of
   so summation-order rounding alone reaches 3.7e-10 there (median 2.6e-14;
   B200, c4).
 * Mixed precision: about three times the maxima and medians measured on a
-  B200 (c3: acc/jrk/snp max 3.1e-7 / 5.6e-6 / 6.3e-5, median 2.0e-8 /
-  1.4e-7 / 2.8e-7; c4: max 2.2e-7 / 3.9e-6 / 1.2e-5 / 4.9e-3, median
-  1.9e-8 / 1.3e-7 / 2.8e-7 / 3.7e-7).  The median bound is what catches a
-  broken accumulation of a derivative; the maxima sit at the particles whose
-  sums cancel.
+  B200 (c1: acc/jrk max 1.07e-6 / 3.5e-6, median 3.2e-8 / 1.5e-7; c2: max
+  1.39e-6 / 4.5e-6, median 2.1e-8 / 1.4e-7; c3: acc/jrk/snp max 3.1e-7 /
+  5.6e-6 / 6.3e-5, median 2.0e-8 / 1.4e-7 / 2.8e-7; c4: max 2.2e-7 /
+  3.9e-6 / 1.2e-5 / 4.9e-3, median 1.9e-8 / 1.3e-7 / 2.8e-7 / 3.7e-7).
+  The median bound is what catches a broken accumulation of a derivative;
+  the maxima sit at the particles whose sums cancel.  Over every particle
+  (c1, c2) the acceleration passes 1e-6 where one close neighbour's pull is
+  about ten times the particle's total force: the FP32 rounding of that one
+  pair term (~1e-7) is then ~1e-6 of the total.
 """
 import numpy as np
 import pytest
@@ -37,9 +41,9 @@ NSAMPLE = {"c1": 1024, "c2": 65536, "c3": 4096, "c4": 4096}   # c1, c2: every pa
 # acc, jrk, snp [, crk]
 FP64_TOL = (1e-12, 1e-12, 1e-12, 1e-9)
 FP64_MEDIAN = 1e-13
-MIXED_TOL = {"c1": (1e-6, 1e-5), "c2": (1e-6, 1e-5),
+MIXED_TOL = {"c1": (3.5e-6, 1.2e-5), "c2": (4e-6, 1.5e-5),
              "c3": (1e-6, 2e-5, 2e-4), "c4": (1e-6, 1.2e-5, 4e-5, 1.5e-2)}
-MIXED_MEDIAN = {"c1": (1e-7, 5e-7), "c2": (1e-7, 5e-7),
+MIXED_MEDIAN = {"c1": (1e-7, 4.5e-7), "c2": (6e-8, 4.5e-7),
                 "c3": (6e-8, 5e-7, 1e-6), "c4": (6e-8, 5e-7, 1e-6, 1.2e-6)}
 T_RUN = {"c1": 1.0 / 64, "c2": 1.0 / 1024, "c3": 1.0 / 1024, "c4": 1.0 / 4096}
 
@@ -69,6 +73,7 @@ def test_sample_against_oracle(name, precision, oracle):
     assert np.all(np.isfinite(got))
     err = rel_err(got, ref)
     print(f"{name} {precision}: max", " ".join(f"{e:.2e}" for e in err.max(axis=0)),
+          "p99", " ".join(f"{e:.2e}" for e in np.quantile(err, 0.99, axis=0)),
           "median", " ".join(f"{e:.2e}" for e in np.median(err, axis=0)))
     for k in range(err.shape[1]):
         tol = FP64_TOL[k] if precision == "fp64" else MIXED_TOL[name][k]
