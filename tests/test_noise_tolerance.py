@@ -152,3 +152,34 @@ def test_split_velocities_do_not_change_fp32_errors(oracle):
         med0, med1 = err[0][0][k], err[1][0][k]
         assert abs(med1 - med0) <= 0.15 * med0, (k, med0, med1)
         assert err[1][1][k] >= 0.5 * err[0][1][k], (k, err[0][1][k], err[1][1][k])
+
+
+def test_fp32_acceleration_error_follows_the_sum_condition(oracle):
+    """The FP32 pair arithmetic's acceleration error at a particle is bounded
+    by the condition number of its force sum, kappa = sum_j |t_j| / |sum_j t_j|
+    (t_j the pair terms), times a few FP32 roundings: the errors above 5e-7
+    sit at particles with kappa >= 5, where a close neighbour's pull is
+    largely cancelled by the rest.  4th order, Plummer N = 16384,
+    eps = 1/1024 (c2's softening)."""
+    import ctypes
+    import numpy as np
+    from hermite_b200.ic import plummer, records
+    lib = _fp32pair_lib()
+    order, n, eps2 = 4, 16384, (1 / 1024) ** 2
+    pred = np.ascontiguousarray(oracle.predict(order, records(plummer(n, 0), order), 0.0))
+    ref = oracle.force(order, pred, n, eps2)
+    got = np.empty_like(ref)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.fp32pair_force(order, n, pred.ctypes.data_as(dp), n, eps2, 0, got.ctypes.data_as(dp))
+    anorm = np.linalg.norm(ref[:, :3], axis=1)
+    err = np.linalg.norm(got[:, :3] - ref[:, :3], axis=1) / anorm
+    assert np.median(err) < 5e-8
+    worst = np.argsort(err)[::-1][:40]
+    assert err[worst[0]] > 5e-7
+    for i in worst:
+        d = pred[:, :3] - pred[i, :3]
+        r2 = (d * d).sum(1) + eps2
+        kappa = (pred[:, 3] * np.sqrt((d * d).sum(1)) / r2 ** 1.5).sum() / anorm[i]
+        assert err[i] <= 2e-7 * kappa, (i, err[i], kappa)
+        if err[i] > 5e-7:
+            assert kappa >= 5.0, (i, err[i], kappa)
