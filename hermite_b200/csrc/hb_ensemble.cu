@@ -91,14 +91,19 @@ struct EnsLaunch {
 };
 
 // j-slices of one i-tile of a cluster with cnt active slots in npad slots:
-// a function of the cluster alone (up to 16 slices when it has few active
-// tiles, none thinner than 4 chunks), so that a cluster's forces -- and its
-// block steps -- do not depend on the other clusters of the ensemble.
+// a function of the cluster alone (up to kEnsSplit (tile, slice) items when
+// it has few active tiles, no slice thinner than 4 chunks), so that a
+// cluster's forces -- and its block steps -- do not depend on the other
+// clusters of the ensemble.  Measured on the batched-ensemble shapes (256
+// clusters, N 1024..32768, 6th order): 16 / 32 / 64 / 128 / 256 items gave
+// 179 / 190 / 194 / 196 / 197 Gint/s; steps with few active particles fill
+// the GPU only with fine slices.
+constexpr int kEnsSplit = 128;
 __device__ __forceinline__ int ens_split(int cnt, int npad)
 {
     const int tiles = (cnt + 31) / 32;
     if (tiles == 0) return 0;
-    return max(1, min(16 / tiles, npad / 128));
+    return max(1, min(kEnsSplit / tiles, npad / 128));
 }
 
 // 1. next block time; reset the per-cluster counters
@@ -889,8 +894,8 @@ int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_
         off += k.npad;
     }
     const size_t ns = e->nslot;
-    // a cluster with j-split tiles has at most 16 (tile, slice) items
-    e->partial_cap = (size_t)16 * nclusters * 32 * e->F;
+    // a cluster with j-split tiles has at most kEnsSplit (tile, slice) items
+    e->partial_cap = (size_t)kEnsSplit * nclusters * 32 * e->F;
     bool ok = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc((void **)&e->d_jp, ns * e->R * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_dt, ns * sizeof(double)) == cudaSuccess &&
