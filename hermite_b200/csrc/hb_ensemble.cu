@@ -7,7 +7,9 @@
 // with inert padding (zero mass, far-away positions, dt = +inf, so never
 // active and contributing exactly zero).  Per block step, all on the device
 // and replayed from a captured CUDA graph:
-//   1. tnext = min over all slots of (tlast + dt); per-cluster counters reset
+//   1. tnext = min over all slots of (tlast + dt), from a compact per-slot
+//      copy the corrector keeps (the records are 112..208 bytes a slot);
+//      per-cluster counters reset
 //   2. active slots compacted into their cluster's own slot range
 //      (ilist[off_c + k]), then one CTA turns the per-cluster counts into
 //      i-tile offsets
@@ -77,6 +79,7 @@ struct EnsSched {
 
 struct EnsLaunch {
     double *jp, *dt, *force, *partial;
+    double *tn;                        // per slot tlast + dt (a compact copy for steps 1, 2a)
     int *ilist, *ccnt, *tile_base;     // tile_base[nclusters + 1]
     int *item_base, *pitem_base;       // per-cluster force items / partial slots, prefix sums
     unsigned *counter;
@@ -111,10 +114,9 @@ template <int ORDER>
 __global__ void ens_min_kernel(EnsLaunch L)
 {
     pdl_enter();
-    constexpr int R = Rec<ORDER>::words;
     double m = __longlong_as_double((long long)kInf);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.nslot; i += gridDim.x * blockDim.x)
-        m = fmin(m, L.dt[i] + L.jp[(size_t)i * R + 7]);
+        m = fmin(m, L.tn[i]);
     for (int o = 16; o; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
     __shared__ double wm[32];
     if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
@@ -134,7 +136,6 @@ template <int ORDER>
 __global__ void ens_compact_kernel(EnsLaunch L)
 {
     pdl_enter();
-    constexpr int R = Rec<ORDER>::words;
     const double tnext = __longlong_as_double((long long)L.s->tnext_bits);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         double dtlim = L.s->dtmax, q = tnext / L.s->dtmax;
@@ -149,7 +150,7 @@ __global__ void ens_compact_kernel(EnsLaunch L)
     for (int base = blockIdx.x * blockDim.x; base < L.nslot; base += gridDim.x * blockDim.x) {
         const int i = base + threadIdx.x;   // blockDim 128: one cluster per block
         const int c = L.slot_cluster[base / kClusterPad];
-        const bool act = i < L.nslot && L.dt[i] + L.jp[(size_t)i * R + 7] == tnext;
+        const bool act = i < L.nslot && L.tn[i] == tnext;
         const unsigned ballot = __ballot_sync(0xffffffffu, act);
         int off = 0;
         if ((threadIdx.x & 31) == 0 && ballot) off = atomicAdd(&L.ccnt[c], __popc(ballot));
@@ -462,6 +463,7 @@ __global__ void ens_correct_kernel(EnsLaunch L)
                                                    etapow, dtlim);
         if (!(dtn >= 0x1p-48)) L.s->error = 1;
         L.dt[i] = dtn;
+        L.tn[i] = L.jp[(size_t)i * R + 7] + dtn;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (L.s->nact > 0) L.s->tsys = L.s->tnext;
@@ -485,6 +487,17 @@ __global__ void ens_all_active_kernel(EnsLaunch L)
         if (threadIdx.x == 0) L.ccnt[c] = cl.n;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) L.s->work = 0;
+}
+
+// tn = tlast + dt for every slot (padding: dt = +inf), before a run of the
+// lockstep engine: the team engine and the host set-up write records and dt
+// without it
+template <int ORDER>
+__global__ void ens_tn_kernel(EnsLaunch L)
+{
+    constexpr int R = Rec<ORDER>::words;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.nslot; i += gridDim.x * blockDim.x)
+        L.tn[i] = L.dt[i] + L.jp[(size_t)i * R + 7];
 }
 
 template <int ORDER>
@@ -615,7 +628,7 @@ struct hb_ens {
     int order = 0, precision = 0, nclusters = 0, nslot = 0, R = 0, F = 0, nsm = 0;
     std::vector<Cluster> cl;
     cudaStream_t stream = nullptr;
-    double *d_jp = nullptr, *d_dt = nullptr, *d_force = nullptr, *d_partial = nullptr,
+    double *d_jp = nullptr, *d_dt = nullptr, *d_tn = nullptr, *d_force = nullptr, *d_partial = nullptr,
            *d_pot = nullptr, *h_eout = nullptr, *d_eout = nullptr;
     int *d_ilist = nullptr, *d_ccnt = nullptr, *d_tile_base = nullptr, *d_slot_cluster = nullptr;
     int *d_item_base = nullptr, *d_pitem_base = nullptr;
@@ -827,6 +840,7 @@ int hb_ens_destroy(hb_ens *e)
     if (e->graph) cudaGraphDestroy(e->graph);
     cudaFree(e->d_jp);
     cudaFree(e->d_dt);
+    cudaFree(e->d_tn);
     cudaFree(e->d_force);
     cudaFree(e->d_partial);
     cudaFree(e->d_pot);
@@ -899,6 +913,7 @@ int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_
     bool ok = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc((void **)&e->d_jp, ns * e->R * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_dt, ns * sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void **)&e->d_tn, ns * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_force, ns * e->F * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_partial, e->partial_cap * sizeof(double)) == cudaSuccess &&
               cudaMalloc((void **)&e->d_pot, ns * sizeof(double)) == cudaSuccess &&
@@ -951,6 +966,7 @@ int hb_ens_create(int order, int nclusters, const int *sizes, int precision, hb_
     EnsLaunch &L = e->L;
     L.jp = e->d_jp;
     L.dt = e->d_dt;
+    L.tn = e->d_tn;
     L.force = e->d_force;
     L.partial = e->d_partial;
     L.ilist = e->d_ilist;
@@ -1130,6 +1146,16 @@ int hb_ens_run(hb_ens *e, double tend, long long max_block_steps)
     if (!(tend >= st->tsys)) return ens_fail(e, HB_ERR_INVALID, "tend is before tsys");
     ce = cudaMemcpy(&e->d_s->tend, &tend, sizeof(double), cudaMemcpyHostToDevice);
     if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "tend upload", ce);
+    {
+        const int nb = std::max(1, std::min((e->nslot + 255) / 256, e->nsm * 8));
+        switch (e->order) {
+        case 4: ens_tn_kernel<4><<<nb, 256, 0, e->stream>>>(e->L); break;
+        case 6: ens_tn_kernel<6><<<nb, 256, 0, e->stream>>>(e->L); break;
+        default: ens_tn_kernel<8><<<nb, 256, 0, e->stream>>>(e->L); break;
+        }
+        ce = cudaGetLastError();
+        if (ce != cudaSuccess) return ens_fail(e, HB_ERR_CUDA, "tlast + dt", ce);
+    }
     long long last = st->block_steps;
     const long long first = st->block_steps;
     while (st->tsys < tend) {
