@@ -759,7 +759,7 @@ def device_integrator_leg(configs=("c1", "c2", "c3")):
     per block step, particle steps x N / time, and the energy error.  c1
     (N = 1024) runs on both engines: "team" (one thread-block cluster, the
     whole loop in one kernel; the automatic choice at this N) and "graph"
-    (four kernels per step over the whole GPU, 32 steps per CUDA-graph
+    (four phases, five kernels, per step over the whole GPU, 32 steps per CUDA-graph
     replay; the automatic choice for c2 and c3) and "persistent" (the same
     phases in one cooperative kernel, grid barriers between them).  c2 and c3
     run windows (t = 0..1/64 and 0..1/32)."""

@@ -4,7 +4,7 @@
 // next block time and the active set (calc_dtlim / count_nact over a
 // dt-sorted array, SRC/nbodysystem.h:652-690), calls the force calculator,
 // corrects the active particles and re-sorts them (:693-765).  Here the whole
-// step stays on the device, four kernels per step, replayed from a captured
+// step stays on the device, four phases per step, replayed from a captured
 // CUDA graph (no host round trip per step):
 //   1. next block time  = min over slots of (tlast + dt)   (grid reduction)
 //   2. active set       = slots with tlast + dt == tnext    (compaction),

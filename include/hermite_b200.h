@@ -188,7 +188,7 @@ int hb_force_variant_info(int order, int precision, int variant,
 int hb_integrator_init(hb_ctx *ctx, double tsys, double eps2, double eta, double eta_s,
                        double dtmax);
 /* Engines for hb_integrator_run (same state, same algorithm):
- *  HB_ENGINE_GRAPH  four kernels per block step over the whole GPU, 32 steps
+ *  HB_ENGINE_GRAPH  four phases (five kernels) per block step over the whole GPU, 32 steps
  *                   per replay of a CUDA graph (any N, FP64 or mixed);
  *  HB_ENGINE_PERSISTENT  the graph engine's phases in one cooperative kernel
  *                   whose CTAs all stay resident, grid barriers (bounded
