@@ -167,17 +167,19 @@ cudaError_t launch_force_lanes(int order, const ForceArgs &a, int nsm, cudaStrea
     // j-slices of at least two chunks a warp, at most two CTAs per SM
     const int S = std::max(1, std::min(2 * nsm, a.nchunk / (2 * kLanesWarps)));
     const dim3 grid(S), block(kLanesWarps * 32);
+    // groups of G = 2..32 lanes (nact <= 16 leaves at least two lanes per i)
+    static_assert(kLanesMaxAct <= 16, "one lane per i-particle is the tiled kernel's job");
     using K = void (*)(ForceArgs);
-    static const K table[3][6] = {
-        {force_lanes_kernel<4, 0>, force_lanes_kernel<4, 1>, force_lanes_kernel<4, 2>,
-         force_lanes_kernel<4, 3>, force_lanes_kernel<4, 4>, force_lanes_kernel<4, 5>},
-        {force_lanes_kernel<6, 0>, force_lanes_kernel<6, 1>, force_lanes_kernel<6, 2>,
-         force_lanes_kernel<6, 3>, force_lanes_kernel<6, 4>, force_lanes_kernel<6, 5>},
-        {force_lanes_kernel<8, 0>, force_lanes_kernel<8, 1>, force_lanes_kernel<8, 2>,
-         force_lanes_kernel<8, 3>, force_lanes_kernel<8, 4>, force_lanes_kernel<8, 5>}};
+    static const K table[3][5] = {
+        {force_lanes_kernel<4, 1>, force_lanes_kernel<4, 2>, force_lanes_kernel<4, 3>,
+         force_lanes_kernel<4, 4>, force_lanes_kernel<4, 5>},
+        {force_lanes_kernel<6, 1>, force_lanes_kernel<6, 2>, force_lanes_kernel<6, 3>,
+         force_lanes_kernel<6, 4>, force_lanes_kernel<6, 5>},
+        {force_lanes_kernel<8, 1>, force_lanes_kernel<8, 2>, force_lanes_kernel<8, 3>,
+         force_lanes_kernel<8, 4>, force_lanes_kernel<8, 5>}};
     const int oi = order == 4 ? 0 : order == 6 ? 1 : order == 8 ? 2 : -1;
     if (oi < 0) return cudaErrorInvalidValue;
-    table[oi][log2g]<<<grid, block, 0, s>>>(a);
+    table[oi][log2g - 1]<<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
 
