@@ -729,8 +729,12 @@ def run_profile_case(case: str):
     fp64_o6_c3 / mixed_o6_c3 = the headline force kernel and its mixed
     counterpart (6th order, N = 262144: 42 MB of records, 0.1-0.25 s per
     launch); the others at N = 65536; team_c1 = one team-kernel launch on c1
-    (N = 1024, 16 CTAs, t = 0..1/128)."""
+    (N = 1024, 16 CTAs, t = 0..1/128); ensemble_window = the ensemble leg's
+    256 clusters on the lockstep engine, t = 0..1/128."""
     from hermite_b200 import Gravity
+    if case == "ensemble_window":
+        print("profile case ensemble_window done", json.dumps(ensemble_leg(tend=1.0 / 128)))
+        return
     if case == "team_c1":
         from hermite_b200.ic import plummer, records
         with Gravity(4, 1024, "fp64") as g:
@@ -894,7 +898,7 @@ def main():
                     help="omit the accuracy, 8th-order, noise and predictor legs")
     ap.add_argument("--skip-integrator", action="store_true",
                     help="omit the device-integrator block-step leg")
-    ap.add_argument("--profile", choices=(*PROFILE_CASES, "team_c1"),
+    ap.add_argument("--profile", choices=(*PROFILE_CASES, "team_c1", "ensemble_window"),
                     help="run one case for an ncu capture and exit")
     args = ap.parse_args()
     if args.profile:
