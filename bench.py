@@ -406,7 +406,11 @@ def run_ours(args):
     traffic = traffic_from_profiles("force_fp64_o6_n262144.txt")
     mtraffic = traffic_from_profiles("force_mixed_o6_n262144.txt")
 
-    accuracy = accuracy_leg("c3") if not args.skip_mixed else None
+    # the accuracy, 8th-order, integrator, ensemble and CPU legs run on
+    # single-GPU runs only (replicas add nothing to them)
+    skip_mixed = args.skip_mixed or world > 1
+    skip_integrator = args.skip_integrator or world > 1
+    accuracy = accuracy_leg("c3") if not skip_mixed else None
     mixed = {
         "value": mvalue, "unit": UNIT, "ms_per_step": sum(mstep_ms) / args.steps,
         "speedup_vs_fp64": mvalue / value * world, "force_ms": mforce_avg_ms,
@@ -418,20 +422,20 @@ def run_ours(args):
                      "peak_source": "packed-FP32 (f32x2) FMA-chain kernel measured in this run"},
         "force_error_vs_oracle": accuracy,
     }
-    c4 = config_c4_leg() if not args.skip_mixed else None
-    noise = noise_leg(accuracy) if not args.skip_mixed else None
-    integ = device_integrator_leg() if not args.skip_integrator else None
-    mixed_int = mixed_integration_leg() if not args.skip_integrator else None
-    ref_gpu = reference_gpu_leg() if not args.skip_integrator else None
-    ens = ensemble_leg() if not args.skip_integrator else None
-    ens_small = small_ensemble_leg() if not args.skip_integrator else None
-    pred = predictor_leg() if not args.skip_mixed else None
+    c4 = config_c4_leg() if not skip_mixed else None
+    noise = noise_leg(accuracy) if not skip_mixed else None
+    integ = device_integrator_leg() if not skip_integrator else None
+    mixed_int = mixed_integration_leg() if not skip_integrator else None
+    ref_gpu = reference_gpu_leg() if not skip_integrator else None
+    ens = ensemble_leg() if not skip_integrator else None
+    ens_small = small_ensemble_leg() if not skip_integrator else None
+    pred = predictor_leg() if not skip_mixed else None
 
     if rank != 0:
         dist_barrier(world)
         return
     cpu = None
-    if not args.skip_cpu:
+    if not args.skip_cpu and world == 1:
         try:
             from oracle import ref_available
             if ref_available("avx", ORDER):
@@ -444,7 +448,7 @@ def run_ours(args):
             cpu = {"value": None, "unit": UNIT, "cores": host_threads(), "kind": "reference",
                    "sample": f"failed: {e}"}
     ens_cpu = None
-    if not args.skip_cpu and not args.skip_integrator:
+    if not args.skip_cpu and not skip_integrator:
         try:
             ens_cpu = ensemble_cpu_leg()
         except Exception as e:
