@@ -205,6 +205,59 @@ __device__ __forceinline__ void chunk64(const double *cp, const Body64 (&I)[NI],
     }
 }
 
+// Small blocks (FP64): the lanes of a warp form groups of G = 2^LOG2G lanes;
+// the lanes of group p share i-particle p and lane g of the group adds
+// j = g, g + G, ... of the chunk.  lanes_log2g picks G = 32 / P for P = nact
+// rounded up to a power of two (nact <= 16, so G >= 2).
+__host__ __device__ __forceinline__ int lanes_log2g(int nact)
+{
+    int lg = 5;
+    while ((1 << (5 - lg)) < nact) --lg;
+    return lg;
+}
+
+template <int ORDER, int LOG2G>
+__device__ __forceinline__ void chunk64_lanes(const double *cp, const Body64 &I, double eps2,
+                                              double (&f)[Frc<ORDER>::words])
+{
+    constexpr int G = 1 << LOG2G, P = 32 / G;
+    const int g = threadIdx.x & (G - 1);
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        Body64 J;
+        load_i64<ORDER>(cp, 0, g + k * G, J);
+        interact64<ORDER>(I, J, eps2, f);
+    }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void chunk64_lanes(int log2g, const double *cp, const Body64 &I,
+                                              double eps2, double (&f)[Frc<ORDER>::words])
+{
+    switch (log2g) {
+    case 1: chunk64_lanes<ORDER, 1>(cp, I, eps2, f); break;
+    case 2: chunk64_lanes<ORDER, 2>(cp, I, eps2, f); break;
+    case 3: chunk64_lanes<ORDER, 3>(cp, I, eps2, f); break;
+    case 4: chunk64_lanes<ORDER, 4>(cp, I, eps2, f); break;
+    default: chunk64_lanes<ORDER, 5>(cp, I, eps2, f); break;
+    }
+}
+
+// After the j sums of a small block: the G lanes of each group add theirs in
+// a fixed butterfly, then lane p takes group p's sum (lanes p >= 32/G keep
+// group 0's), so the results sit where the one-i-per-lane code has them.
+template <int F>
+__device__ __forceinline__ void lanes_gather(int log2g, double (&f)[F])
+{
+    const int G = 1 << log2g, lane = threadIdx.x & 31;
+    for (int o = G >> 1; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < F; ++q) f[q] += __shfl_xor_sync(0xffffffffu, f[q], o);
+    const int src = (lane < (32 >> log2g) ? lane : 0) << log2g;
+#pragma unroll
+    for (int q = 0; q < F; ++q) f[q] = __shfl_sync(0xffffffffu, f[q], src);
+}
+
 template <int ORDER, int NI, bool REFINE>
 __device__ __forceinline__ void chunk_mixed(const float *cp, const NegI32 (&I)[NI], float2 eps2,
                                             double (&f)[NI][Frc<ORDER>::words])

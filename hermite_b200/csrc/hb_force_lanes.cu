@@ -65,7 +65,7 @@ template <int ORDER, int LOG2G>
 __global__ void __launch_bounds__(kLanesWarps * 32)
 force_lanes_kernel(ForceArgs a)
 {
-    constexpr int G = 1 << LOG2G, P = 32 / G;
+    constexpr int G = 1 << LOG2G;
     constexpr int F = Frc<ORDER>::words, NC = Pred64<ORDER>::ncomp;
     // per warp: one predicted chunk; after the j loop the same space holds
     // the warps' group sums, then the cross-slice group sums
@@ -95,12 +95,7 @@ force_lanes_kernel(ForceArgs a)
     for (int c = c0 + w; c < c1; c += kLanesWarps) {
         predict_chunk_warp<ORDER>(a.jp, c, a.nbody, a.tsys, my);
         __syncwarp();
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            Body64 J;
-            load_i64<ORDER>(my, 0, g + k * G, J);
-            interact64<ORDER>(I, J, a.eps2, f);
-        }
+        chunk64_lanes<ORDER, LOG2G>(my, I, a.eps2, f);
         __syncwarp();
     }
     // the G lanes of a group: a fixed butterfly
@@ -162,8 +157,7 @@ force_lanes_kernel(ForceArgs a)
 cudaError_t launch_force_lanes(int order, const ForceArgs &a, int nsm, cudaStream_t s)
 {
     if (a.nact < 1 || a.nact > kLanesMaxAct || a.nchunk < 1) return cudaErrorInvalidValue;
-    int log2g = 5;
-    while ((1 << (5 - log2g)) < a.nact) --log2g;          // P = 2^(5 - log2g) >= nact
+    const int log2g = lanes_log2g(a.nact);                // P = 2^(5 - log2g) >= nact
     // j-slices of at least two chunks a warp, at most two CTAs per SM
     const int S = std::max(1, std::min(2 * nsm, a.nchunk / (2 * kLanesWarps)));
     const dim3 grid(S), block(kLanesWarps * 32);

@@ -227,6 +227,10 @@ __device__ __forceinline__ bool items_phase(const ItemsArgs &a, unsigned char *s
     while (S > 1 && (size_t)S * gx * TI * F > a.partial_cap) --S;
     const int items = gx * S;
     const size_t ispan = (size_t)gx * TI;
+    // FP64 steps of at most kLanesMaxAct active slots: lanes share an
+    // i-particle and split each chunk's j (lanes_log2g, hb_force.cuh)
+    constexpr bool kLaneSplit = !MIXED && ORDER != 9;
+    const int lg = kLaneSplit && nact <= kLanesMaxAct ? lanes_log2g(nact) : 0;
 
     const float2 eps2f = f2((float)eps2);
     for (;;) {
@@ -249,7 +253,7 @@ __device__ __forceinline__ bool items_phase(const ItemsArgs &a, unsigned char *s
         using IBody = typename std::conditional<MIXED, NegI32, Body64>::type;
         IBody I[1];
         if constexpr (MIXED) load_i_mixed<ORDER>(reinterpret_cast<const float *>(ptile), 0, lane, I[0]);
-        else load_i64<ORDER>(reinterpret_cast<const double *>(ptile), 0, lane, I[0]);
+        else load_i64<ORDER>(reinterpret_cast<const double *>(ptile), 0, lg ? min(lane >> lg, nact - 1) : lane, I[0]);
         __syncthreads();
 
         double f[1][F], tot[1][F], cmp[1][F];   // FP64: per-tile sums, Kahan-folded
@@ -280,10 +284,14 @@ __device__ __forceinline__ bool items_phase(const ItemsArgs &a, unsigned char *s
             __syncthreads();
             if (tid == 0 && t + STG < ntile) issue(t + STG);
             for (int q = jg; q < cnt; q += WJ) {
-                if constexpr (MIXED)
+                if constexpr (MIXED) {
                     chunk_mixed<ORDER, 1, (HB_MIXED_REFINE != 0)>(reinterpret_cast<const float *>(ptile + q * CB), I, eps2f, f);
-                else
-                    chunk64<ORDER, 1>(reinterpret_cast<const double *>(ptile + q * CB), I, eps2, f);
+                } else {
+                    if (kLaneSplit && lg)
+                        chunk64_lanes<ORDER>(lg, reinterpret_cast<const double *>(ptile + q * CB), I[0], eps2, f[0]);
+                    else
+                        chunk64<ORDER, 1>(reinterpret_cast<const double *>(ptile + q * CB), I, eps2, f);
+                }
             }
             if constexpr (kKahan<ORDER, MIXED>) kahan_fold<1, F>(tot, cmp, f);
             __syncthreads();
@@ -302,6 +310,7 @@ __device__ __forceinline__ bool items_phase(const ItemsArgs &a, unsigned char *s
 #pragma unroll
             for (int c = 0; c < F; ++c) f[0][c] = __dsub_rn(tot[0][c], cmp[0][c]);
         }
+        if (kLaneSplit && lg) lanes_gather<F>(lg, f[0]);
 
         // the 4 warps' j quarters, in warp order
         double *red = reinterpret_cast<double *>(smem);
@@ -397,6 +406,10 @@ __device__ __forceinline__ bool big_phase(const ItemsArgs &a, unsigned char *sme
     while (S > 1 && (size_t)S * gx * TI * F > a.partial_cap) --S;
     const int items = gx * S;
     const size_t ispan = (size_t)gx * TI;
+    // FP64 steps of at most kLanesMaxAct active slots: lanes share an
+    // i-particle and split each chunk's j (lanes_log2g, hb_force.cuh)
+    constexpr bool kLaneSplit = !MIXED && ORDER != 9;
+    const int lg = kLaneSplit && nact <= kLanesMaxAct ? lanes_log2g(nact) : 0;
 
     const float2 eps2f = f2((float)eps2);
     for (;;) {
