@@ -73,3 +73,20 @@ def test_slice_candidates():
         c = autotune.s_candidates(nact, 65536, 148, 128)
         assert c == sorted(set(c)) and c[0] == 1
         assert all(1 <= s <= 65536 // 256 for s in c)
+
+
+def test_bench_reads_the_tiled_shape_the_library_takes():
+    """bench.py's comparison runs of the tiled kernel use the tuning table's
+    shape for the bucket (nearest N, then nearest nact; slice count rescaled
+    to the bucket's CTA count), as the library's automatic choice does."""
+    import sys
+    sys.path.insert(0, str(autotune.PKG.parent))
+    import bench
+    table = {e[:4]: e[4:] for e in _entries(TABLE)}
+    for nact in (1, 4, 16):
+        v, s = bench.tiled_shape(6, 262144, nact)
+        la = min((k[3] for k in table if k[:3] == (6, 0, 18)), key=lambda b: abs(b - math.log2(nact)))
+        tv, ts = table[(6, 0, 18, la)]
+        assert v == tv
+        # one i-tile at these nact: the slice count scales by the bucket's i-tiles
+        assert s >= ts and s % ts == 0
