@@ -734,8 +734,20 @@ def run_profile_case(case: str):
     counterpart (6th order, N = 262144: 42 MB of records, 0.1-0.25 s per
     launch); the others at N = 65536; team_c1 = one team-kernel launch on c1
     (N = 1024, 16 CTAs, t = 0..1/128); ensemble_window = the ensemble leg's
-    256 clusters on the lockstep engine, t = 0..1/128."""
+    256 clusters on the lockstep engine, t = 0..1/128; lanes_o6_c3 = three
+    block steps of one active particle at N = 262144 (the small-step kernel)."""
     from hermite_b200 import Gravity
+    if case == "lanes_o6_c3":
+        # the small-step kernel: nact = 1 against N = 262144 (6th order, FP64)
+        g = Gravity(6, 262144, "fp64")
+        g.set_jp_records(plummer_records(6, 262144))
+        out = np.empty((1, 9))
+        for k in range(3):
+            g.predict_all(1e-6 * k)
+            g.calc_force_on_first_nact(1, EPS * EPS, out)
+        g.close()
+        print("profile case lanes_o6_c3 done")
+        return
     if case == "ensemble_window":
         print("profile case ensemble_window done", json.dumps(ensemble_leg(tend=1.0 / 128)))
         return
@@ -902,7 +914,7 @@ def main():
                     help="omit the accuracy, 8th-order, noise and predictor legs")
     ap.add_argument("--skip-integrator", action="store_true",
                     help="omit the device-integrator block-step leg")
-    ap.add_argument("--profile", choices=(*PROFILE_CASES, "team_c1", "ensemble_window"),
+    ap.add_argument("--profile", choices=(*PROFILE_CASES, "team_c1", "ensemble_window", "lanes_o6_c3"),
                     help="run one case for an ncu capture and exit")
     args = ap.parse_args()
     if args.profile:
