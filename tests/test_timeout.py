@@ -43,3 +43,25 @@ def test_wait_timeout_reported_and_context_recovers(order, precision, variant, j
     err = rel_err(got, ref)
     assert err[:, 0].max() <= TOL[precision], err.max(axis=0)
     assert (got == again).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", [4, 6, 8])
+def test_small_step_kernel_wait_timeout(order, oracle):
+    """The small-step kernel (automatic shape, FP64, nact <= 16) waits on the
+    bulk copies of each warp's raw chunks with the same bounded waits: with
+    the limit at 0 the call reports HB_ERR_DEVICE_TIMEOUT, and the context
+    then gives the oracle's forces."""
+    n, nact = 20000, 3
+    rec = make_records(order, n, seed=23 + order)
+    ref = oracle.predict_force(order, rec, 0.0, nact, EPS2)
+    with hb.Gravity(order, n, "fp64") as g:
+        g.set_jp_records(rec)
+        g.predict_all(0.0)
+        g.set_wait_limit(0)
+        with pytest.raises(hb.HermiteError) as ei:
+            g.calc_force_on_first_nact(nact, EPS2)
+        assert ei.value.status == HB_ERR_DEVICE_TIMEOUT
+        g.set_wait_limit(-1)
+        got = g.calc_force_on_first_nact(nact, EPS2)
+    assert rel_err(got, ref).max() <= TOL["fp64"]
