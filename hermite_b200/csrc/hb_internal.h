@@ -143,7 +143,8 @@ const ForceVariant *force_variant(int order, bool mixed, int v);
 // FP64 force for block steps of at most kLanesMaxAct active particles
 // (orders 4, 6, 8): lanes of a warp share an i-particle and split j
 // (hb_force_lanes.cu).  Uses a.jp / a.tsys / a.nbody (it predicts the raw
-// records itself), a.partial for S * kLanesMaxAct * F doubles and a.counter[0].
+// records itself), a.partial for S * kLanesMaxAct * F doubles, a.counter[0],
+// and a.spin / a.err for its bounded waits on bulk copies.
 constexpr int kLanesMaxAct = 16;
 cudaError_t launch_force_lanes(int order, const ForceArgs &a, int nsm, cudaStream_t s);
 
